@@ -1,0 +1,228 @@
+/*
+ * lbflow.h -- C ABI of the B200 lattice Boltzmann engine (liblbflow_b200.so).
+ *
+ * The reference crate (gilberto-ribeiro/lbflow, pure Rust, CPU only) has no FFI:
+ * its public entry point is `lbflow::solve(momentum::Parameters,
+ * Option<Vec<passive_scalar::Parameters>>)` (src/lib.rs:170-191), which builds a
+ * `momentum::Lattice` (src/momentum/lattice.rs:27-207), initialises it
+ * (src/momentum/lattice.rs:322-328) and loops `main_steps` + residuals + stop
+ * (src/momentum.rs:262-293, src/passive_scalar.rs:136-177).  This header splits
+ * that monolithic call into the pieces a Rust `extern "C"` facade (or ctypes /
+ * cgo / JNI) binds: a domain descriptor that mirrors `momentum::Parameters`,
+ * a scalar descriptor that mirrors `passive_scalar::Parameters`, and
+ * create / init / step / residual / observe / destroy calls.  Every call returns
+ * an lbf_status and never aborts; lbf_last_error() gives the message of the
+ * last failure on the calling thread.
+ *
+ * Conventions
+ *  - Node index i = x + nx*(y + ny*z), as in src/momentum/lattice.rs:70-84.
+ *  - All host arrays are owned by the caller; the library copies what it needs.
+ *    Device memory is owned by the library behind the opaque handles.
+ *  - A domain handle is not thread-safe; distinct handles may be used from
+ *    distinct threads.
+ *  - `stream` arguments are cudaStream_t passed as void* (NULL = legacy stream).
+ */
+#ifndef LBFLOW_B200_H
+#define LBFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBF_ABI_VERSION 1
+
+typedef enum {
+    LBF_OK = 0,
+    LBF_EINVAL = 1,      /* bad descriptor or argument (reference: panic!)      */
+    LBF_ENOMEM = 2,      /* device or host allocation failed / no room in batch  */
+    LBF_EDEVICE = 3,     /* CUDA error                                           */
+    LBF_ETIMEOUT = 4,    /* a bounded wait ran out                               */
+    LBF_ENAN = 5,        /* non-finite value detected in a reduction             */
+    LBF_EUNSUPPORTED = 6,/* valid in the reference model, not built on device    */
+    LBF_ESTATE = 7       /* call out of order (e.g. step before init)            */
+} lbf_status;
+
+/* velocity_set::VelocitySet discriminants (src/velocity_set.rs:19-25). */
+enum { LBF_D2Q5 = 0, LBF_D2Q9 = 1, LBF_D3Q15 = 2, LBF_D3Q19 = 3, LBF_D3Q27 = 4 };
+
+/* BoundaryFace discriminants (src/lib.rs:17-25). */
+enum { LBF_WEST = 0, LBF_EAST = 1, LBF_SOUTH = 2, LBF_NORTH = 3, LBF_BOTTOM = 4, LBF_TOP = 5 };
+
+/* CollisionOperator::{BGK(tau), TRT(omega_plus, omega_minus), MRT(rates)} (src/lib.rs:37-42). */
+enum { LBF_BGK = 0, LBF_TRT = 1, LBF_MRT = 2 };
+
+/* momentum::bc::BoundaryCondition (src/momentum/bc.rs:12-26). */
+enum {
+    LBF_BC_NO_SLIP = 0,
+    LBF_BC_BOUNCE_BACK = 1,      /* moving wall: density, velocity          */
+    LBF_BC_ANTI_BOUNCE_BACK = 2, /* pressure: density                       */
+    LBF_BC_ZOU_HE = 3,           /* Option<density>, Vec<Option<velocity>>  */
+    LBF_BC_PERIODIC = 4
+};
+
+/* passive_scalar::bc::BoundaryCondition (src/passive_scalar/bc.rs:9-29). */
+enum {
+    LBF_SBC_ANTI_BOUNCE_BACK = 0,     /* Dirichlet: scalar_value             */
+    LBF_SBC_ANTI_BB_NO_FLUX = 1,
+    LBF_SBC_BB_NO_FLUX = 2,
+    LBF_SBC_ZEROTH_ORDER_NO_FLUX = 3, /* unknown_populations_only            */
+    LBF_SBC_SECOND_ORDER_NO_FLUX = 4, /* unknown_populations_only            */
+    LBF_SBC_PERIODIC = 5
+};
+
+/* passive_scalar::bc::InnerBoundaryCondition (src/passive_scalar/bc.rs:31-35). */
+enum { LBF_INNER_ANTI_BOUNCE_BACK = 0, LBF_INNER_BOUNCE_BACK = 1 };
+
+/* Population storage on the device.  Collision arithmetic runs in FP64 for
+ * LBF_STORE_F64 and in FP32 for the other three.  The *_DEV formats store the
+ * deviation f_i - w_i (momentum) in 16 bits. */
+enum { LBF_STORE_F64 = 0, LBF_STORE_F32 = 1, LBF_STORE_F16DEV = 2, LBF_STORE_BF16DEV = 3 };
+
+/* LBF_COMPAT_REFERENCE reproduces the reference arithmetic exactly, including
+ * its quirks (force only in BGK collision, src/momentum/node.rs:311-333; the MRT
+ * equilibrium-moment functions of src/velocity_set/d2q9.rs:247-264 and
+ * src/velocity_set/d3q19.rs:550-587).  LBF_COMPAT_PHYSICS adds the Guo source
+ * term to TRT/MRT and uses m_eq = M f_eq. */
+enum { LBF_COMPAT_REFERENCE = 0, LBF_COMPAT_PHYSICS = 1 };
+
+/* Node class bits returned by lbf_domain_get_node_class (exact-parity masks). */
+#define LBF_CLASS_SOLID       0x1u   /* NodeType::Solid (src/lib.rs:31-35)                     */
+#define LBF_CLASS_BOUNCE_BACK 0x2u   /* fluid node with a solid neighbour (lattice.rs:177-191) */
+#define LBF_CLASS_FACE_SHIFT  2      /* bit 2+f: fluid node on face f (lattice.rs:163-175)     */
+
+typedef struct {
+    int32_t kind;                 /* LBF_BGK / LBF_TRT / LBF_MRT                      */
+    int32_t _pad;
+    double tau;                   /* BGK(tau)                                         */
+    double omega_plus;            /* TRT(omega_plus, omega_minus): relaxation rates   */
+    double omega_minus;
+    double relaxation[27];        /* MRT(relaxation_vector), length Q                 */
+} lbf_collision_desc;
+
+typedef struct {
+    int32_t kind;                 /* LBF_BC_*                                         */
+    int32_t has_density;          /* ZouHe: Some(density) ; BounceBack/AntiBB: used   */
+    double density;
+    int32_t has_velocity[3];      /* ZouHe: Some(u_x) ...                             */
+    int32_t _pad;
+    double velocity[3];           /* BounceBack / ZouHe wall velocity                 */
+} lbf_bc_desc;
+
+/* Mirrors momentum::Parameters (src/momentum.rs:22-37).  The force closure is a
+ * constant body force; NodeTypes is a uint8 mask (0 fluid, 1 solid, the map.xyz
+ * tokens of src/io.rs:88-96); InitialDensity/InitialVelocity are uniform values
+ * or per-node arrays. */
+typedef struct {
+    int32_t velocity_set;         /* LBF_D2Q9 / LBF_D3Q19 / LBF_D3Q27                 */
+    int32_t storage;              /* LBF_STORE_*                                      */
+    int64_t n[3];                 /* n[2] ignored for 2-D sets                        */
+    lbf_collision_desc collision;
+    int32_t has_force;            /* Some(force)                                      */
+    int32_t compat;               /* LBF_COMPAT_*                                     */
+    double force[3];
+    lbf_bc_desc bc[6];            /* indexed by face (LBF_WEST..LBF_TOP)              */
+    int32_t face_order[6];        /* order in which face BCs run; all zero = W,E,S,N,B,T */
+    const uint8_t* node_type;     /* N entries or NULL (= NodeTypes::OnlyFluidNodes)  */
+    double initial_density;       /* InitialDensity::Uniform                          */
+    double initial_velocity[3];   /* InitialVelocity::Uniform                         */
+    const double* initial_density_field;   /* N entries or NULL                       */
+    const double* initial_velocity_field;  /* N*D entries ([node][d]) or NULL         */
+} lbf_domain_desc;
+
+typedef struct {
+    int32_t kind;                 /* LBF_SBC_*                                        */
+    int32_t unknown_populations_only;
+    double scalar_value;          /* AntiBounceBack { scalar_value }                  */
+} lbf_scalar_bc_desc;
+
+/* Mirrors passive_scalar::Parameters (src/passive_scalar.rs:16-25) and
+ * adsorption::Parameters with AdsorptionModel::Langmuir
+ * (src/passive_scalar/adsorption.rs:4-28). */
+typedef struct {
+    int32_t velocity_set;
+    int32_t inner_boundary_condition;     /* LBF_INNER_*                              */
+    lbf_collision_desc collision;
+    int32_t has_source;                   /* Some(source_value) (constant)            */
+    int32_t has_adsorption;
+    double source_value;
+    double initial_scalar_value;          /* InitialScalarValue::Uniform              */
+    const double* initial_scalar_field;   /* N entries or NULL                        */
+    lbf_scalar_bc_desc bc[6];
+    double adsorption_rate;               /* k_a                                      */
+    double desorption_rate;               /* k_d                                      */
+    double q_max;
+    double initial_q_ads;
+} lbf_scalar_desc;
+
+typedef struct lbf_domain lbf_domain;
+
+/* ---- library ----------------------------------------------------------- */
+int32_t     lbf_abi_version(void);
+const char* lbf_last_error(void);
+/* sizeof() of the descriptor structs, so bindings can check their layouts. */
+size_t      lbf_sizeof(int32_t which);   /* 0 domain_desc, 1 scalar_desc, 2 bc_desc, 3 collision_desc */
+
+/* Velocity-set tables as built on the device side (src/velocity_set.rs:28-190):
+ * c[q*3], w[q], q_bar[q], q_faces[6*9] (-1 padded), face_normal[6],
+ * mrt[q*q], mrt_inverse[q*q].  Any pointer may be NULL. */
+lbf_status lbf_velocity_set_tables(int32_t velocity_set, int32_t* d, int32_t* q,
+                                   int32_t* c, double* w, int32_t* q_bar,
+                                   int32_t* q_faces, int32_t* face_normal,
+                                   double* mrt, double* mrt_inverse);
+
+/* ---- one domain (replaces momentum::Lattice + passive_scalar::Lattice) ---- */
+/* Lattice::new (src/momentum/lattice.rs:27-207). */
+lbf_status lbf_domain_create(const lbf_domain_desc* desc, lbf_domain** out);
+/* passive_scalar::Lattice::new (src/passive_scalar/lattice.rs:26-181). One scalar per domain. */
+lbf_status lbf_scalar_attach(lbf_domain* dom, const lbf_scalar_desc* desc);
+/* Lattice::initialize_nodes (src/momentum/lattice.rs:322-328,
+ * src/passive_scalar/lattice.rs:241-246): f = f_eq(rho0, u0) on fluid nodes. */
+lbf_status lbf_domain_init(lbf_domain* dom, void* stream);
+/* nsteps x main_steps (src/momentum/lattice.rs:431-441 then
+ * src/passive_scalar/lattice.rs:342-350), asynchronous on `stream`.  With
+ * residual_interval k > 0, the residuals of every step t with t % k == 0 are
+ * computed (compute_lattice_residuals, src/momentum/lattice.rs:369-394). */
+lbf_status lbf_domain_step(lbf_domain* dom, int64_t nsteps, int64_t residual_interval, void* stream);
+/* The driver loop of src/momentum.rs:262-293: step until
+ * (t > 10 and all residuals <= tolerance) or t > max_iterations.  Residuals are
+ * checked every `residual_interval` steps (1 = the reference).  Writes the number
+ * of main_steps executed to *steps_done.  Synchronous. */
+lbf_status lbf_domain_run(lbf_domain* dom, int64_t max_iterations, int64_t residual_interval,
+                          double tolerance_density, double tolerance_velocity,
+                          double tolerance_scalar, int64_t* steps_done, void* stream);
+/* Residuals of the last residual step: [density, velocity_x.., scalar] (1+D+S entries).
+ * Synchronous.  *time_step receives the step they belong to (-1 if none yet). */
+lbf_status lbf_domain_residuals(lbf_domain* dom, double* out, int64_t* time_step);
+/* Moments at the current time step (what write_data stores in data/<t>/,
+ * src/momentum/io.rs:74-192): density[N], velocity[N*D], scalar[N] (host
+ * pointers, any may be NULL).  Solid nodes report their initial values. */
+lbf_status lbf_domain_get_moments(lbf_domain* dom, double* density, double* velocity,
+                                  double* scalar, void* stream);
+/* Adsorbed amount q_ads per node (0 where not a bounce-back node). Host pointer. */
+lbf_status lbf_domain_get_q_ads(lbf_domain* dom, double* q_ads);
+/* FP64 inventories over fluid nodes: [sum rho, sum rho*u (D), sum C, sum q_ads]. */
+lbf_status lbf_domain_inventory(lbf_domain* dom, double* out, void* stream);
+/* Node classes (LBF_CLASS_* bits) and solid-neighbour link masks (bit i: the
+ * neighbour along c_i is solid), computed on the device. */
+lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint32_t* links);
+/* Number of main_steps executed so far (the reference's time_step). */
+lbf_status lbf_domain_time_step(lbf_domain* dom, int64_t* t);
+/* Device bytes held by the domain. */
+lbf_status lbf_domain_device_bytes(lbf_domain* dom, int64_t* bytes);
+lbf_status lbf_domain_destroy(lbf_domain* dom);
+
+/* ---- whole solve with host buffers (the `lbflow::solve` drop-in) --------- */
+/* Creates a domain from `desc` (+ optional scalar), initialises it, runs
+ * `nsteps` main_steps and copies the final moments to the host arrays.
+ * Host->device and device->host copies are part of the call. */
+lbf_status lbf_solve(const lbf_domain_desc* desc, const lbf_scalar_desc* scalar,
+                     int64_t nsteps, double* density, double* velocity, double* scalar_out,
+                     void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBFLOW_B200_H */
