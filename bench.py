@@ -1,0 +1,296 @@
+"""Benchmark: MLUPS and HBM-roofline fraction of the fused LB step, D3Q19 TRT
+porous channel 256^3 (FP32 storage), the headline configuration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--storage f32|f16dev|bf16dev|f64] [--n 256]
+
+One step = one main_steps over the whole lattice (one fused kernel launch).
+Inputs are resident in HBM (2 x 19 x 4 B x 16.8 M nodes = 2.5 GB of populations,
+far larger than the 126 MB L2, so no flush is needed between steps).  `e2e` is
+the same metric through lbf_solve with host buffers (mask upload, init, K steps
+and the moment download inside the timed region).  Under torchrun each rank
+advances its own copy of the domain (weak scaling, no data-path collective);
+timing is the max over ranks of CUDA-event time on the launching stream.
+
+--impl reference times the CPU oracle (a restatement of the reference's Rust
+step, OpenMP over all host cores) on the same geometry.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STORAGE = {"f64": 0, "f32": 1, "f16dev": 2, "bf16dev": 3}
+SBYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--storage", default="f32", choices=list(STORAGE))
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--block", type=int, default=0, help="override the x block size")
+    return ap.parse_args()
+
+
+def geometry(n: int, seed: int) -> np.ndarray:
+    from lbflow_b200.cases import sphere_pack
+    cache = os.path.join(tempfile.gettempdir(), "lbflow_b200_cache")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, f"spheres_{n}_{seed}_p070_r4-10.npy")
+    if os.path.exists(path):
+        return np.load(path)
+    mask = sphere_pack([n, n, n], 0.7, 4.0, 10.0, seed)
+    np.save(path, mask)
+    return mask
+
+
+def params_for(args, mask):
+    from lbflow_b200 import cases
+    from lbflow_b200.core import Storage
+    return cases.porous_channel_d3q19([args.n] * 3, mask=mask, force=1e-6, storage=Storage(STORAGE[args.storage]))
+
+
+def workload_name(args):
+    return (f"D3Q19 TRT porous channel {args.n}^3 (tau+=0.8, magic 1/4, g_x=1e-6, spheres r in [4,10], "
+            f"porosity 0.7, periodic x, no-slip y/z)")
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.path = os.path.join(tempfile.gettempdir(), f"lbf_clocks_{os.getpid()}.csv")
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax.append(float(p[2]))
+                except ValueError:
+                    continue
+                for k, nm in enumerate(names):
+                    if p[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def profile_traffic(storage: str, n: int):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"d3q19_trt_porous_step_{storage}.md")
+    if not os.path.exists(path):
+        return None
+    with open(path) as fh:
+        m = re.search(rf"traffic_bytes_per_launch_{n}:\s*([0-9.eE+]+)", fh.read())
+    return float(m.group(1)) if m else None
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline(args, mask, steps=3):
+    """The oracle on the full lattice for a few main_steps on all host cores."""
+    from lbflow_b200 import momentum as m
+    from oracle import oracle as orc
+    p = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
+    desc, keep = m.to_desc(p)
+    od = orc.Domain(desc, keep=keep).init()
+    od.step(1)
+    t0 = time.perf_counter()
+    od.step(steps)
+    dt = time.perf_counter() - t0
+    return {"value": od.num_fluid * steps / dt / 1e6, "unit": "MLUPS", "cores": orc.num_threads(), "kind": "port",
+            "sample": f"oracle (FP64 CPU restatement) on the same {args.n}^3 lattice, {steps} main_steps after "
+                      f"1 warm-up, {orc.num_threads()} OpenMP threads"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    mask = geometry(args.n, args.seed)
+    from lbflow_b200 import momentum as m
+    from oracle import oracle as orc
+    p = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
+    desc, keep = m.to_desc(p)
+    od = orc.Domain(desc, keep=keep).init()
+    warm = min(args.warmup, 2)
+    od.step(warm)
+    k = max(1, min(args.steps, 8))   # bounded sample: a few full-lattice steps
+    t0 = time.perf_counter()
+    od.step(k)
+    dt = time.perf_counter() - t0
+    mlups = od.num_fluid * k / dt / 1e6
+    cores = orc.num_threads()
+    sample = (f"oracle (FP64 CPU restatement of the reference step) on the {args.n}^3 lattice, {k} main_steps timed "
+              f"after {warm} warm-up, {cores} OpenMP threads (the Rust reference cannot be built here)")
+    line = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world,
+            "steps": k, "warmup": warm, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere packing)",
+            "config": {"workload": workload_name(args), "storage": "f64 (CPU)"},
+            "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from lbflow_b200 import _abi
+    from lbflow_b200.domain import Domain, solve_arrays
+
+    torch.cuda.set_device(local_rank)
+    mask = geometry(args.n, args.seed)
+    p = params_for(args, mask)
+    n_fluid = int(np.count_nonzero(mask == 0))
+    N = mask.size
+    stream = torch.cuda.current_stream()
+    dom = Domain(p)
+    if args.block:
+        pass
+    dom.init(stream)
+    dom.step(args.warmup, 0, stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        start.record(stream)
+        dom.step(args.steps, 0, stream)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = clk.summary()
+    sec = ms / 1e3
+    mlups = world * n_fluid * args.steps / sec / 1e6
+    # roofline of the step kernel (one launch per step)
+    s = SBYTES[args.storage]
+    alg_bytes = n_fluid * 2 * 19 * s + N * 1   # read + write Q populations per fluid node + 1 B node type
+    per_launch = sec / args.steps
+    achieved = alg_bytes / per_launch / 1e9
+    peak, peak_kind = peaks()
+    traffic = profile_traffic(args.storage, args.n)
+    # end to end through lbf_solve with host buffers
+    e2e = None
+    if not args.no_e2e:
+        del dom
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        wall0 = time.perf_counter()
+        solve_arrays(p, args.steps, stream=stream)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        e_ms = t0.elapsed_time(t1)
+        e_sec = max(e_ms / 1e3, wall)
+        if world > 1:
+            t = torch.tensor([e_sec], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_sec = float(t.item())
+        e2e = {"value": world * n_fluid * args.steps / e_sec / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": N / args.steps, "d2h_bytes_per_step": N * 4 * 8 / args.steps,
+               "note": "lbf_solve: node-type upload, init, K steps, density+velocity download (FP64) per solve"}
+    if rank != 0:
+        return
+    base = None if args.no_cpu_baseline else cpu_baseline(args, mask)
+    line = {"metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64",
+            "data": "synthetic (seeded sphere packing)",
+            "config": {"workload": workload_name(args), "storage": args.storage, "n_fluid": n_fluid,
+                       "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "engine":
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_engine(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

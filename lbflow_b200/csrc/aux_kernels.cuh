@@ -1,0 +1,176 @@
+// aux_kernels.cuh -- node classification, initialisation and FP64 reductions.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace lbf {
+
+struct SetupParams {
+    int nx, ny, nz, pad;
+    long long N;
+    const uint8_t* type;      // 0 fluid, 1 solid
+    uint32_t* cls;            // LBF_CLASS_* bits
+    uint32_t* links;          // bit i: neighbour along c_i is solid
+    uint32_t* mask;           // kernel mask word (M_* bits)
+    unsigned fold_faces;      // faces whose no-slip walls fold into the link bits
+    unsigned explicit_faces;  // faces whose BCs run explicitly (M_FACE)
+    unsigned skip_faces;      // faces updated by the face pass (M_SKIP)
+    unsigned pad2;
+    unsigned long long* counts;   // [0] fluid nodes, [1] bounce-back nodes
+};
+
+// Lattice::new node classification (src/momentum/lattice.rs:156-191): fluid
+// nodes, face membership of fluid nodes, and bounce-back nodes with the
+// directions whose (periodic) neighbour is solid.
+template <int VS>
+__global__ void k_setup(const SetupParams S) {
+    using L = Lat<VS>;
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (cell >= S.N) return;
+    const int x = (int)(cell % S.nx);
+    const int y = (int)((cell / S.nx) % S.ny);
+    const int z = (int)(cell / ((long long)S.nx * S.ny));
+    if (S.type[cell]) {
+        S.cls[cell] = 1u;
+        S.links[cell] = 0u;
+        S.mask[cell] = M_SOLID;
+        return;
+    }
+    uint32_t links = 0u;
+    sfor<L::Q>([&](auto I) {
+        constexpr int i = I;
+        int xx = x + L::c(i, 0), yy = y + L::c(i, 1), zz = z + (L::D == 3 ? L::c(i, 2) : 0);
+        xx = xx < 0 ? xx + S.nx : (xx >= S.nx ? xx - S.nx : xx);
+        yy = yy < 0 ? yy + S.ny : (yy >= S.ny ? yy - S.ny : yy);
+        zz = zz < 0 ? zz + S.nz : (zz >= S.nz ? zz - S.nz : zz);
+        const long long n = (long long)xx + (long long)S.nx * ((long long)yy + (long long)S.ny * zz);
+        if (S.type[n]) links |= 1u << i;
+    });
+    uint32_t cls = links ? 2u : 0u;
+    uint32_t mask = links | (links ? M_BB : 0u);
+    const int on[6] = {x == 0, x == S.nx - 1, y == 0, y == S.ny - 1, z == 0, z == S.nz - 1};
+    sfor<L::NF>([&](auto FF) {
+        constexpr int F = FF;
+        if (on[F]) {
+            cls |= 1u << (2 + F);
+            if (S.fold_faces >> F & 1u) {
+                sfor<L::Q>([&](auto I) {
+                    if constexpr (leaves<L>(I, F)) mask |= 1u << int(I);
+                });
+            }
+            if (S.explicit_faces >> F & 1u) mask |= M_FACE;
+            if (S.skip_faces >> F & 1u) mask |= M_SKIP;
+        }
+    });
+    S.cls[cell] = cls;
+    S.links[cell] = links;
+    S.mask[cell] = mask;
+    atomicAdd(&S.counts[0], 1ull);
+    if (links) atomicAdd(&S.counts[1], 1ull);
+}
+
+struct InitParams {
+    double rho0, u0[3], c0, q0;
+    const double* rho_field;   // or null
+    const double* u_field;     // [N][D] or null
+    const double* c_field;     // or null
+};
+
+// Lattice::initialize_nodes (src/momentum/lattice.rs:322-328,
+// src/passive_scalar/lattice.rs:241-246): f = f_eq(rho0, u0), g = g_eq(C0, u0)
+// on fluid nodes, evaluated in FP64 and stored in the storage format.  Also
+// seeds the residual "previous" moments with the initial values (the
+// ShallowNode of src/momentum/node.rs:93-111) and both parities of the
+// face-layer buffers.
+template <int VS, int ST, bool SCALAR>
+__global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, void* pb0_1, void* pb1_0, void* pb1_1,
+                       void* pb2_0, void* pb2_1, void* pb3_0, void* pb3_1, void* pb4_0, void* pb4_1, void* pb5_0,
+                       void* pb5_1) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (cell >= P.N) return;
+    Geo g;
+    g.x = (int)(cell % P.nx);
+    g.y = (int)((cell / P.nx) % P.ny);
+    g.z = (int)(cell / ((long long)P.nx * P.ny));
+    g.cell = cell;
+    const double rho = I0.rho_field ? I0.rho_field[cell] : I0.rho0;
+    double u[3] = {I0.u0[0], I0.u0[1], I0.u0[2]};
+    if (I0.u_field)
+        for (int a = 0; a < D; ++a) u[a] = I0.u_field[cell * D + a];
+    const double c0 = I0.c_field ? I0.c_field[cell] : I0.c0;
+    const uint32_t mk = P.mask[cell];
+    const bool fluid = !(mk & M_SOLID);
+    double uu = 0.0;
+    for (int a = 0; a < D; ++a) uu += u[a] * u[a];
+    if (fluid) {
+        sfor<Q>([&](auto Ii) {
+            constexpr int i = Ii;
+            const double fe = feq_i<L, double>(i, rho, u, uu);
+            S::st(const_cast<void*>(P.srcp[i]), cell, R(fe), R(L::w(i)));
+        });
+        if constexpr (SCALAR) {
+            sfor<Q>([&](auto Ii) {
+                constexpr int i = Ii;
+                ((R*)P.gsrcp[i])[cell] = R(feq_i<L, double>(i, c0, u, uu));
+            });
+            if (P.qads) ((R*)P.qads)[cell] = (mk & M_BB) ? R(I0.q0) : R(0);
+            if (P.cprev) ((R*)P.cprev)[cell] = R(c0);
+        }
+        if (P.mom_prev) {
+            R* mp = (R*)P.mom_prev;
+            mp[cell] = R(rho);
+            for (int a = 0; a < D; ++a) mp[(1 + a) * P.N + cell] = R(u[a]);
+            if (SCALAR) mp[(1 + D) * P.N + cell] = R(c0);
+        }
+    }
+    void* pbs[6][2] = {{pb0_0, pb0_1}, {pb1_0, pb1_1}, {pb2_0, pb2_1}, {pb3_0, pb3_1}, {pb4_0, pb4_1}, {pb5_0, pb5_1}};
+    for (int F = 0; F < L::NF; ++F) {
+        if (!pbs[F][0]) continue;
+        const int dist = face_dist(g, F, P);
+        if (dist > 1) continue;
+        const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+        for (int par = 0; par < 2; ++par) {
+            R* pb = (R*)pbs[F][par];
+            for (int a = 0; a < D; ++a) pb[(dist * (D + 1) + a) * pl + pos] = R(u[a]);
+            pb[(dist * (D + 1) + D) * pl + pos] = R(c0);
+        }
+    }
+}
+
+// Sum the NSLOT partials of each accumulator; out[k] = sqrt(sum) for residuals
+// or the plain sum for inventories; clears the partials for the next use.
+static __global__ void k_finalize(double* accum, int nacc, int take_sqrt, double* out) {
+    const int k = threadIdx.x;
+    if (k >= nacc) return;
+    double s = 0.0;
+    for (int j = 0; j < NSLOT; ++j) {
+        s += accum[j * NACC + k];
+        accum[j * NACC + k] = 0.0;
+    }
+    out[k] = take_sqrt ? sqrt(s) : s;
+}
+
+// FP64 inventories over fluid nodes from observed moments:
+// [sum rho, sum rho*u_a (D), sum C, sum q_ads].
+template <int D, class R>
+__global__ void k_inventory(const uint32_t* mask, long long N, const double* rho, const double* u, const double* c,
+                            const R* qads, double* accum) {
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double vq = 0.0;
+    if (cell < N && !(mask[cell] & M_SOLID)) {
+        v[0] = rho[cell];
+        for (int a = 0; a < D; ++a) v[1 + a] = rho[cell] * u[cell * D + a];
+        if (c) v[1 + D] = c[cell];
+        if (qads) vq = double(qads[cell]);
+    }
+    if (D == 2) v[4] = vq;   // slots: rho, j0, j1, C, q   (2-D)
+    double w[6] = {v[0], v[1], v[2], v[3], v[4], D == 3 ? vq : 0.0};
+    block_accumulate<6>(w, accum);
+}
+
+}  // namespace lbf

@@ -1,0 +1,816 @@
+// kernels.cuh -- the fused lattice Boltzmann step for sm_100a.
+//
+// One kernel advances every fluid node by one reference `main_steps`
+// (src/momentum/lattice.rs:431-441; src/passive_scalar/lattice.rs:342-350):
+//
+//   pull-stream + inner bounce-back + face BCs  ->  f_t        (read Q values)
+//   moments (rho, u with the F/2 shift)         ->  rho_t, u_t
+//   equilibrium + BGK/TRT/MRT (+ Guo source)    ->  f*_t       (write Q values)
+//   [passive scalar: the same on g, Langmuir adsorption, with u_t]
+//
+// State between launches is the post-collision field f*_{t-1} in SoA planes
+// (plane i holds direction i for all nodes, node index x + nx*(y + ny*z)).  The
+// step for time t pulls f_t(x)[i] = f*_{t-1}(x - c_i)[i] with periodic wrap
+// (src/lib.rs:141-152, src/momentum/lattice.rs:127-154), replaces the directions
+// whose neighbour is solid by the node's own reflected value (src/lib.rs:154-165),
+// applies the face BCs in order (src/momentum/bc.rs:29-149), and only then
+// collides.  Two population buffers alternate (A/B): each node's Q values are
+// read once and written once per step, and boundary rules keep the exact
+// reference semantics ("streaming scheme").
+//
+// The step at t = 0 reads f_0 = f_eq(rho0, u0) from the node itself
+// (Lattice::initialize_nodes, src/momentum/lattice.rs:322-328).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+
+namespace lbf {
+
+constexpr int COLL_BGK = 0, COLL_TRT = 1, COLL_MRT = 2;
+constexpr int ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3;
+constexpr int COMPAT_REFERENCE = 0, COMPAT_PHYSICS = 1;
+
+// Per-node mask word.  Bits 0..26: the neighbour along c_i is solid (or, on the
+// lean path, a no-slip wall); bit 27 solid node; bit 28 bounce-back node (has a
+// solid neighbour, drives adsorption); bit 29 node needs explicit face BCs;
+// bit 30 node is updated by the face pass, not by the bulk sweep.
+constexpr uint32_t M_LINKS = (1u << 27) - 1u;
+constexpr uint32_t M_SOLID = 1u << 27;
+constexpr uint32_t M_BB = 1u << 28;
+constexpr uint32_t M_FACE = 1u << 29;
+constexpr uint32_t M_SKIP = 1u << 30;
+
+constexpr int NSLOT = 256;   // partial-sum slots of the FP64 reductions
+constexpr int NACC = 8;      // accumulators per slot
+
+// Boundary-condition kinds: the C-ABI values (include/lbflow.h).
+enum { BC_NO_SLIP = 0, BC_BOUNCE_BACK = 1, BC_ANTI_BB = 2, BC_ZOU_HE = 3, BC_PERIODIC = 4 };
+enum { SBC_ANTI_BB = 0, SBC_ANTI_BB_NO_FLUX = 1, SBC_BB_NO_FLUX = 2, SBC_ZEROTH = 3, SBC_SECOND = 4,
+       SBC_PERIODIC = 5 };
+
+struct FaceBC {
+    int kind, has_rho;
+    int has_u[3];
+    int pad;
+    double rho;
+    double u[3];
+};
+struct SFaceBC {
+    int kind, unknown_only;
+    int given_vel;   // 1: wall velocity from the momentum BC of the face; 0: extrapolate
+    int pad;
+    double value;
+    double u[3];
+};
+
+struct StepParams {
+    int nx, ny, nz, dims;
+    long long N;
+    const uint32_t* mask;
+    const void* srcp[27];   // plane pointers of f*_{t-1} (or f_0 when first)
+    void* dstp[27];         // plane pointers of f*_t
+    int coll, compat, has_force, first;
+    double tau, omega, op, om;
+    double rates[27];
+    double force[3];
+    FaceBC face[6];
+    int order[6];
+    int any_face;
+    int observe, write_mom, residual;
+    // previous-step moments of the two node layers next to each face:
+    // [layer 0/1][field u_0..u_{D-1}, C][plane node], compute type
+    const void* pb_src[6];
+    void* pb_dst[6];
+    long long pb_plane[6];
+    // per-node moments for residuals: [field][N] (rho, u_0.., C), compute type
+    const void* mom_prev;
+    void* mom_cur;
+    double* accum;   // [NSLOT][NACC]
+    double* obs_rho;
+    double* obs_u;
+    double* obs_c;
+    // passive scalar (same velocity set as the momentum lattice)
+    int has_scalar, s_coll, s_inner, s_has_source;
+    double s_tau, s_omega, s_op, s_om, s_source;
+    int s_ads, s_pad0, s_pad1, s_pad2;
+    double ka, kd, qmax;
+    double c_solid;          // initial scalar of solid nodes when uniform
+    const double* c_init;    // per-node initial scalar, or null
+    const void* gsrcp[27];
+    void* gdstp[27];
+    void* qads;              // adsorbed amount per node (compute type), in place
+    void* cprev;             // scalar value of the previous step per node, in place
+    SFaceBC sface[6];
+};
+
+template <int VS>
+struct KParams : StepParams {};
+// D3Q27 MRT: population-space collision matrix Lambda = M^-1 S M, built on the host.
+template <>
+struct KParams<VS_D3Q27> : StepParams {
+    float lam32[27 * 27];
+    double lam64[27 * 27];
+};
+
+// ---- storage formats -----------------------------------------------------
+template <int ST>
+struct Store;
+template <>
+struct Store<ST_F64> {
+    using T = double;
+    using R = double;
+    __device__ static __forceinline__ R ld(const void* p, long long o, R) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ void st(void* p, long long o, R v, R) { ((T*)p)[o] = v; }
+};
+template <>
+struct Store<ST_F32> {
+    using T = float;
+    using R = float;
+    __device__ static __forceinline__ R ld(const void* p, long long o, R) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ void st(void* p, long long o, R v, R) { ((T*)p)[o] = v; }
+};
+// 16-bit deviation formats: the stored value is f_i - w_i.
+template <>
+struct Store<ST_F16> {
+    using T = __half;
+    using R = float;
+    __device__ static __forceinline__ R ld(const void* p, long long o, R w) {
+        return __half2float(((const T*)p)[o]) + w;
+    }
+    __device__ static __forceinline__ void st(void* p, long long o, R v, R w) {
+        ((T*)p)[o] = __float2half_rn(v - w);
+    }
+};
+template <>
+struct Store<ST_BF16> {
+    using T = __nv_bfloat16;
+    using R = float;
+    __device__ static __forceinline__ R ld(const void* p, long long o, R w) {
+        return __bfloat162float(((const T*)p)[o]) + w;
+    }
+    __device__ static __forceinline__ void st(void* p, long long o, R v, R w) {
+        ((T*)p)[o] = __float2bfloat16_rn(v - w);
+    }
+};
+
+// ---- node geometry -----------------------------------------------------------
+struct Geo {
+    int x, y, z;
+    int xm, xp, ym, yp, zm, zp;
+    long long cell;
+    __device__ __forceinline__ long long at(int dx, int dy, int dz, const StepParams& P) const {
+        const int xx = dx < 0 ? xm : (dx > 0 ? xp : x);
+        const int yy = dy < 0 ? ym : (dy > 0 ? yp : y);
+        const int zz = dz < 0 ? zm : (dz > 0 ? zp : z);
+        return (long long)xx + (long long)P.nx * ((long long)yy + (long long)P.ny * zz);
+    }
+};
+
+__device__ __forceinline__ bool on_face(const Geo& g, int f, const StepParams& P) {
+    switch (f) {
+        case 0: return g.x == 0;
+        case 1: return g.x == P.nx - 1;
+        case 2: return g.y == 0;
+        case 3: return g.y == P.ny - 1;
+        case 4: return g.z == 0;
+        default: return g.z == P.nz - 1;
+    }
+}
+__device__ __forceinline__ int face_dist(const Geo& g, int f, const StepParams& P) {
+    switch (f) {
+        case 0: return g.x;
+        case 1: return P.nx - 1 - g.x;
+        case 2: return g.y;
+        case 3: return P.ny - 1 - g.y;
+        case 4: return g.z;
+        default: return P.nz - 1 - g.z;
+    }
+}
+__device__ __forceinline__ long long face_pos(const Geo& g, int f, const StepParams& P) {
+    return f < 2 ? (long long)g.y + (long long)P.ny * g.z
+                 : (f < 4 ? (long long)g.x + (long long)P.nx * g.z : (long long)g.x + (long long)P.nx * g.y);
+}
+
+// ---- reductions ----------------------------------------------------------------
+template <int K>
+__device__ __forceinline__ void block_accumulate(double (&v)[K], double* accum) {
+    __shared__ double red[32][K];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[wid][k] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nw ? red[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) {
+                const unsigned long long b = blockIdx.x + (unsigned long long)gridDim.x *
+                                                              (blockIdx.y + (unsigned long long)gridDim.y * blockIdx.z);
+                atomicAdd(&accum[(b % NSLOT) * NACC + k], s);
+            }
+        }
+    }
+}
+
+// ---- equilibrium (src/kernel.rs:3-26) -------------------------------------------
+template <class L, class R>
+__device__ __forceinline__ R feq_i(int i, R rho, const R* u, R uu) {
+    R cu = R(0);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) cu += u[a] * R(L::c(i, a));
+    return R(L::w(i)) * rho * (R(1) + cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
+}
+
+// Guo source without the (1 - omega/2) factor (src/kernel.rs:122-154).
+template <class L, class R>
+__device__ __forceinline__ R guo_i(int i, const R* u, const R* F) {
+    R cu = R(0);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) cu += u[a] * R(L::c(i, a));
+    R s = R(0);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) s += (R(3) * R(L::c(i, a)) - R(3) * u[a] + R(9) * cu * R(L::c(i, a))) * F[a];
+    return R(L::w(i)) * s;
+}
+
+// Reference MRT equilibrium moments, bug for bug
+// (src/velocity_set/d2q9.rs:247-264, src/velocity_set/d3q19.rs:550-587).
+template <int VS, class R>
+__device__ __forceinline__ void meq_reference(R rho, const R* u, R* m) {
+    if constexpr (VS == VS_D2Q9) {
+        const R s = u[0] * u[0] + u[1] * u[1];
+        m[0] = rho;
+        m[1] = rho - R(3) * rho * s;
+        m[2] = R(9) * rho * u[0] * u[0] * u[1] * u[1] - R(3) * rho * s + rho;
+        m[3] = rho * u[0];
+        m[4] = R(3) * rho * u[0] * u[0] * u[0] - rho * u[0];
+        m[5] = rho * u[1];
+        m[6] = R(3) * rho * u[1] * u[1] * u[1] - rho * u[1];
+        m[7] = rho * s;
+        m[8] = rho * u[0] * u[1];
+    } else if constexpr (VS == VS_D3Q19) {
+        const R s = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+        const R bug = R(2) * rho * u[0] * u[0] - rho * (u[1] * u[1] + u[2] + u[2]);
+        m[0] = rho;
+        m[1] = R(-11) * rho + R(19) * rho * s;
+        m[2] = R(3) * rho - R(5.5) * rho * s;
+        m[3] = rho * u[0];
+        m[4] = R(-2.0 / 3.0) * rho * u[0];
+        m[5] = rho * u[1];
+        m[6] = R(-2.0 / 3.0) * rho * u[1];
+        m[7] = rho * u[2];
+        m[8] = R(-2.0 / 3.0) * rho * u[2];
+        m[9] = bug;
+        m[10] = R(-0.5) * bug;
+        m[11] = rho * (u[1] * u[1] - u[2] * u[2]);
+        m[12] = R(-0.5) * rho * (u[1] * u[1] - u[2] * u[2]);
+        m[13] = rho * u[0] * u[1];
+        m[14] = rho * u[1] * u[2];
+        m[15] = rho * u[0] * u[2];
+        m[16] = R(0);
+        m[17] = R(0);
+        m[18] = R(0);
+    }
+}
+
+template <int VS, class R>
+__device__ __forceinline__ R lam_at(const KParams<VS>& P, int k) {
+    if constexpr (VS == VS_D3Q27) {
+        if constexpr (sizeof(R) == 8) return P.lam64[k];
+        else return P.lam32[k];
+    } else {
+        return R(0);
+    }
+}
+
+// Collision in place on f (registers) given feq; src/kernel.rs:28-120 and the
+// force source of src/momentum/node.rs:311-333 (BGK) / the physics mode.
+template <int VS, int COLL, class R>
+__device__ __forceinline__ void collide(const KParams<VS>& P, R (&f)[Lat<VS>::Q], const R (&fe)[Lat<VS>::Q], R rho,
+                                        const R* u, const R* F, bool force, double tau, double omega,
+                                        double op, double om, const double* rates, int compat) {
+    using L = Lat<VS>;
+    constexpr int Q = L::Q;
+    if constexpr (COLL == COLL_BGK) {
+        const R w1 = R(omega), w0 = R(1) - R(omega);
+        const R cb = R(1.0 - 0.5 / tau);
+        sfor<Q>([&](auto I) {
+            constexpr int i = I;
+            R v = w0 * f[i] + w1 * fe[i];
+            if (force) v += cb * guo_i<L, R>(i, u, F);
+            f[i] = v;
+        });
+    } else if constexpr (COLL == COLL_TRT) {
+        const R wp = R(op), wm = R(om);
+        const bool src = force && compat == COMPAT_PHYSICS;
+        const R cp = R(1.0 - 0.5 * op), cm = R(1.0 - 0.5 * om);
+        R out[Q];
+        sfor<Q>([&](auto I) {
+            constexpr int i = I;
+            constexpr int ib = L::qbar(i);
+            const R fp = R(0.5) * (f[i] + f[ib]), fep = R(0.5) * (fe[i] + fe[ib]);
+            const R fm = R(0.5) * (f[i] - f[ib]), fem = R(0.5) * (fe[i] - fe[ib]);
+            R v = f[i] - wp * (fp - fep) - wm * (fm - fem);
+            if (src) {
+                const R si = guo_i<L, R>(i, u, F), sb = guo_i<L, R>(ib, u, F);
+                v += cp * R(0.5) * (si + sb) + cm * R(0.5) * (si - sb);
+            }
+            out[i] = v;
+        });
+        sfor<Q>([&](auto I) { f[I] = out[I]; });
+    } else {   // MRT
+        if constexpr (VS == VS_D3Q27) {
+            const bool src = force && compat == COMPAT_PHYSICS;
+            R d[Q], s[Q];
+            sfor<Q>([&](auto I) { d[I] = f[I] - fe[I]; });
+            if (src) sfor<Q>([&](auto I) { s[I] = guo_i<L, R>(I, u, F); });
+            sfor<Q>([&](auto I) {
+                constexpr int i = I;
+                R acc = R(0), accs = R(0);
+                sfor<Q>([&](auto J) {
+                    const R lam = lam_at<VS, R>(P, i * Q + J);
+                    acc += lam * d[J];
+                    if (src) accs += lam * s[J];
+                });
+                f[i] = f[i] - acc + (src ? s[i] - R(0.5) * accs : R(0));
+            });
+        } else {
+            R m[Q], me[Q];
+            sfor<Q>([&](auto K) {
+                constexpr int k = K;
+                R a = R(0);
+                sfor<Q>([&](auto I) {
+                    constexpr double c = L::M(k, I);
+                    if constexpr (c != 0.0) a += R(c) * f[I];
+                });
+                m[k] = a;
+            });
+            if (compat == COMPAT_REFERENCE) {
+                meq_reference<VS, R>(rho, u, me);
+            } else {
+                sfor<Q>([&](auto K) {
+                    constexpr int k = K;
+                    R a = R(0);
+                    sfor<Q>([&](auto I) {
+                        constexpr double c = L::M(k, I);
+                        if constexpr (c != 0.0) a += R(c) * fe[I];
+                    });
+                    me[k] = a;
+                });
+            }
+            const bool src = force && compat == COMPAT_PHYSICS;
+            R ms[Q];
+            if (src) {
+                R s[Q];
+                sfor<Q>([&](auto I) { s[I] = guo_i<L, R>(I, u, F); });
+                sfor<Q>([&](auto K) {
+                    constexpr int k = K;
+                    R a = R(0);
+                    sfor<Q>([&](auto I) {
+                        constexpr double c = L::M(k, I);
+                        if constexpr (c != 0.0) a += R(c) * s[I];
+                    });
+                    ms[k] = (R(1) - R(0.5) * R(rates[k])) * a;
+                });
+            }
+            sfor<Q>([&](auto K) {
+                constexpr int k = K;
+                m[k] = m[k] - R(rates[k]) * (m[k] - me[k]) + (src ? ms[k] : R(0));
+            });
+            sfor<Q>([&](auto I) {
+                constexpr int i = I;
+                R a = R(0);
+                sfor<Q>([&](auto K) {
+                    constexpr double c = mrt_inv<L>(i, K);
+                    if constexpr (c != 0.0) a += R(c) * m[K];
+                });
+                f[i] = a;
+            });
+        }
+    }
+}
+
+// D2Q9 Zou-He, src/velocity_set/d2q9.rs:165-245 (formulas verbatim).
+template <class R>
+__device__ __forceinline__ void zou_he_d2q9(int face, R* f, const FaceBC& b) {
+    const bool vel = !b.has_rho;
+    R rho, ux, uy;
+    switch (face) {
+        case 0:
+            uy = R(b.u[1]);
+            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) - ux) * (f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
+            else { rho = R(b.rho); ux = R(1) - R(1) / rho * (f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
+            f[1] = f[3] + R(2.0 / 3.0) * rho * ux;
+            f[5] = f[7] - R(0.5) * (f[2] - f[4]) + R(0.5) * rho * uy + R(1.0 / 6.0) * rho * ux;
+            f[8] = f[6] + R(0.5) * (f[2] - f[4]) - R(0.5) * rho * uy + R(1.0 / 6.0) * rho * ux;
+            break;
+        case 1:
+            uy = R(b.u[1]);
+            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) + ux) * (f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])); }
+            else { rho = R(b.rho); ux = R(1) / rho * (f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])) - R(1); }
+            f[3] = f[1] - R(2.0 / 3.0) * rho * ux;
+            f[7] = f[5] + R(0.5) * (f[2] - f[4]) - R(0.5) * rho * uy - R(1.0 / 6.0) * rho * ux;
+            f[6] = f[8] - R(0.5) * (f[2] - f[4]) + R(0.5) * rho * uy - R(1.0 / 6.0) * rho * ux;
+            break;
+        case 2:
+            ux = R(b.u[0]);
+            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) - uy) * (f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
+            else { rho = R(b.rho); uy = R(1) - R(1) / rho * (f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
+            f[2] = f[4] + R(2.0 / 3.0) * rho * uy;
+            f[5] = f[7] - R(0.5) * (f[1] - f[3]) + R(0.5) * rho * ux + R(1.0 / 6.0) * rho * uy;
+            f[6] = f[8] + R(0.5) * (f[1] - f[3]) - R(0.5) * rho * ux + R(1.0 / 6.0) * rho * uy;
+            break;
+        default:
+            ux = R(b.u[0]);
+            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) + uy) * (f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])); }
+            else { rho = R(b.rho); uy = R(1) / rho * (f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])) - R(1); }
+            f[4] = f[2] - R(2.0 / 3.0) * rho * uy;
+            f[7] = f[5] + R(0.5) * (f[1] - f[3]) - R(0.5) * rho * ux - R(1.0 / 6.0) * rho * uy;
+            f[8] = f[6] - R(0.5) * (f[1] - f[3]) + R(0.5) * rho * ux - R(1.0 / 6.0) * rho * uy;
+            break;
+    }
+}
+
+// D3Q19 Zou-He (engine extension; the reference has none): Hecht & Harting (2010).
+template <class L, int F, class R>
+__device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b) {
+    constexpr int ax = F / 2;
+    constexpr int sgn = (F & 1) ? -1 : 1;   // inward normal sign along ax
+    R s0 = R(0), sout = R(0);
+    sfor<L::Q>([&](auto I) {
+        constexpr int cn = L::c(I, ax) * sgn;
+        if constexpr (cn == 0) s0 += f[I];
+        else if constexpr (cn < 0) sout += f[I];
+    });
+    R u[3] = {R(0), R(0), R(0)};
+    R rho;
+    if (!b.has_rho) {
+        u[0] = R(b.u[0]); u[1] = R(b.u[1]); u[2] = R(b.u[2]);
+        rho = (s0 + R(2) * sout) / (R(1) - R(sgn) * u[ax]);
+    } else {
+        rho = R(b.rho);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) if (a != ax) u[a] = R(b.u[a]);
+        u[ax] = R(sgn) * (R(1) - (s0 + R(2) * sout) / rho);
+    }
+    R N[3] = {R(0), R(0), R(0)};
+    sfor<3>([&](auto A) {
+        if constexpr (A != ax) {
+            R s = R(0);
+            sfor<L::Q>([&](auto I) {
+                if constexpr (L::c(I, ax) == 0 && L::c(I, A) != 0) s += R(L::c(I, A)) * f[I];
+            });
+            N[A] = R(0.5) * s - rho * u[A] / R(3);
+        }
+    });
+    sfor<L::Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (L::c(i, ax) * sgn == 1) {
+            R cu = R(0), ct = R(0);
+            sfor<3>([&](auto A) {
+                cu += R(L::c(i, A)) * u[A];
+                if constexpr (A != ax) ct += R(L::c(i, A)) * N[A];
+            });
+            f[i] = f[L::qbar(i)] + R(6.0 * L::w(i)) * rho * cu - ct;
+        }
+    });
+}
+
+// Face BCs on the momentum populations of a node on face F
+// (src/momentum/bc.rs:62-149), after streaming and inner bounce-back.
+template <int VS, int ST, int F>
+__device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g, typename Store<ST>::R* f) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    const FaceBC& b = P.face[F];
+    const int kind = b.kind;
+    if (kind == BC_PERIODIC) return;
+    if (kind == BC_NO_SLIP || kind == BC_BOUNCE_BACK) {
+        const R rw = R(b.rho);
+        sfor<L::Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (leaves<L>(i, F)) {
+                R v = S::ld(P.srcp[i], g.cell, R(L::w(i)));
+                if (kind == BC_BOUNCE_BACK) {
+                    R cu = R(0);
+#pragma unroll
+                    for (int a = 0; a < L::D; ++a) cu += R(b.u[a]) * R(L::c(i, a));
+                    v = v - R(2) * R(L::w(i)) * rw * R(3) * cu;
+                }
+                f[L::qbar(i)] = v;
+            }
+        });
+    } else if (kind == BC_ANTI_BB) {
+        // wall velocity 1.5 u(x) - 0.5 u(x + n) from the previous step (bc.rs:86-117)
+        const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+        const R* pb = (const R*)P.pb_src[F];
+        R uw[3] = {R(0), R(0), R(0)};
+#pragma unroll
+        for (int a = 0; a < L::D; ++a)
+            uw[a] = R(1.5) * pb[(0 * (L::D + 1) + a) * pl + pos] - R(0.5) * pb[(1 * (L::D + 1) + a) * pl + pos];
+        R uu = R(0);
+#pragma unroll
+        for (int a = 0; a < L::D; ++a) uu += uw[a] * uw[a];
+        const R rw = R(b.rho);
+        sfor<L::Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (leaves<L>(i, F)) {
+                R cu = R(0);
+#pragma unroll
+                for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
+                f[L::qbar(i)] = -S::ld(P.srcp[i], g.cell, R(L::w(i))) +
+                                R(2) * R(L::w(i)) * rw * (R(1) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
+            }
+        });
+    } else if (kind == BC_ZOU_HE) {
+        if constexpr (VS == VS_D2Q9) zou_he_d2q9<R>(F, f, b);
+        else if constexpr (VS == VS_D3Q19) zou_he_3d<L, F, R>(f, b);
+    }
+}
+
+// Scalar face BCs (src/passive_scalar/bc.rs:37-152).  Extrapolation outflow
+// (zeroth / second order) is applied by the face pass.
+template <int VS, int F, class R>
+__device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, R* gg) {
+    using L = Lat<VS>;
+    const SFaceBC& b = P.sface[F];
+    const int kind = b.kind;
+    if (kind == SBC_PERIODIC || kind == SBC_ZEROTH || kind == SBC_SECOND) return;
+    if (kind == SBC_BB_NO_FLUX) {
+        sfor<L::Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (leaves<L>(i, F)) gg[L::qbar(i)] = ((const R*)P.gsrcp[i])[g.cell];
+        });
+        return;
+    }
+    // anti-bounce-back with the wall equilibrium (bc.rs:107-140)
+    const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+    const R* pb = (const R*)P.pb_src[F];
+    R uw[3] = {R(0), R(0), R(0)};
+    if (b.given_vel) {
+#pragma unroll
+        for (int a = 0; a < L::D; ++a) uw[a] = R(b.u[a]);
+    } else {
+#pragma unroll
+        for (int a = 0; a < L::D; ++a)
+            uw[a] = R(1.5) * pb[(0 * (L::D + 1) + a) * pl + pos] - R(0.5) * pb[(1 * (L::D + 1) + a) * pl + pos];
+    }
+    const R sval = kind == SBC_ANTI_BB ? R(b.value) : pb[(0 * (L::D + 1) + L::D) * pl + pos];
+    R uu = R(0);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) uu += uw[a] * uw[a];
+    sfor<L::Q>([&](auto I) {
+        constexpr int i = I;
+        if constexpr (leaves<L>(i, F)) {
+            R cu = R(0);
+#pragma unroll
+            for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
+            const R ge = R(L::w(i)) * sval * (R(1) + cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
+            gg[L::qbar(i)] = -((const R*)P.gsrcp[i])[g.cell] + R(2) * ge;
+        }
+    });
+}
+
+// Apply the face BCs of a node in the configured order (P.order).
+template <int VS, int ST, bool SCALAR>
+__device__ __forceinline__ void apply_faces(const KParams<VS>& P, const Geo& g, typename Store<ST>::R* f,
+                                            typename Store<ST>::R* gg) {
+    using L = Lat<VS>;
+    using R = typename Store<ST>::R;
+    sfor<L::NF>([&](auto O) {
+        const int fr = P.order[O];
+        sfor<L::NF>([&](auto FF) {
+            constexpr int F = FF;
+            if (fr == F && on_face(g, F, P)) {
+                momentum_face<VS, ST, F>(P, g, f);
+                if constexpr (SCALAR) scalar_face<VS, F, R>(P, g, gg);
+            }
+        });
+    });
+}
+
+// Scalar source of one node (src/passive_scalar/node.rs:258-266 with
+// src/passive_scalar/adsorption.rs:50-92).  Updates q when `commit`.
+template <class R>
+__device__ __forceinline__ bool scalar_source(const StepParams& P, bool bb, R c_stored, R& q, bool commit, R& out) {
+    if (!P.s_ads) {
+        out = R(P.s_source);
+        return P.s_has_source != 0;
+    }
+    R ads = R(0);
+    if (bb) {
+        const R r = R(P.ka) * c_stored * (R(P.qmax) - q) - R(P.kd) * q;
+        ads = -r;
+        if (commit) {
+            R qn = q + r;
+            if (qn < R(0)) qn = R(0);
+            else if (qn > R(P.qmax)) qn = R(P.qmax);
+            q = qn;
+        }
+    }
+    out = P.s_has_source ? R(P.s_source) + ads : ads;
+    return true;
+}
+
+// =================================================================== the step
+// MODE: 0 bulk sweep (skips nodes of the face pass), 1 face pass.
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+
+    Geo g;
+    g.x = blockIdx.x * blockDim.x + threadIdx.x;
+    g.y = blockIdx.y;
+    g.z = blockIdx.z;
+    const bool inside = g.x < P.nx;
+    g.cell = (long long)(inside ? g.x : 0) + (long long)P.nx * ((long long)g.y + (long long)P.ny * g.z);
+    const uint32_t mk = inside ? P.mask[g.cell] : M_SOLID;
+    const bool active = !(mk & M_SOLID);
+
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+        g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+        g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+        g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+        g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+        g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+
+        // ---- stream (pull) + inner bounce-back -------------------------------
+        R f[Q];
+        if (P.first) {
+            sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], g.cell, R(L::w(I))); });
+        } else {
+            sfor<Q>([&](auto I) {
+                constexpr int i = I, ib = L::qbar(i);
+                if (mk >> ib & 1u) {
+                    f[i] = S::ld(P.srcp[ib], g.cell, R(L::w(ib)));
+                } else {
+                    const long long n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
+                    f[i] = S::ld(P.srcp[i], n, R(L::w(i)));
+                }
+            });
+        }
+        // scalar populations: pull + inner BC (src/passive_scalar/lattice.rs:274-297)
+        R gg[SCALAR ? Q : 1];
+        if constexpr (SCALAR) {
+            if (P.first) {
+                sfor<Q>([&](auto I) { gg[I] = ((const R*)P.gsrcp[I])[g.cell]; });
+            } else {
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    const long long n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
+                    if (mk >> ib & 1u) {
+                        const R own = ((const R*)P.gsrcp[ib])[g.cell];
+                        if (P.s_inner == 1) {
+                            gg[i] = own;   // InnerBounceBack
+                        } else {           // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
+                            const R cs = P.c_init ? R(P.c_init[n]) : R(P.c_solid);
+                            gg[i] = -own + R(2) * R(L::w(ib)) * cs;
+                        }
+                    } else {
+                        gg[i] = ((const R*)P.gsrcp[i])[n];
+                    }
+                });
+            }
+        }
+        // ---- face boundary conditions ------------------------------------------
+        if constexpr (FACEBC) {
+            if (!P.first && (mk & M_FACE)) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+        }
+
+        // ---- moments (src/momentum/node.rs:418-457) ------------------------------
+        R rho = R(0);
+        sfor<Q>([&](auto I) { rho += f[I]; });
+        R u[3] = {R(0), R(0), R(0)};
+        sfor<D>([&](auto A) {
+            R s = R(0);
+            sfor<Q>([&](auto I) {
+                constexpr int c = L::c(I, A);
+                if constexpr (c == 1) s += f[I];
+                else if constexpr (c == -1) s -= f[I];
+            });
+            u[A] = s / rho;
+        });
+        R F[3] = {R(P.force[0]), R(P.force[1]), R(P.force[2])};
+        const bool force = P.has_force != 0;
+        if (force) sfor<D>([&](auto A) { u[A] += R(0.5) * F[A] / rho; });
+
+        // ---- scalar value (src/passive_scalar/node.rs:272-279) --------------------
+        R cval = R(0), q = R(0), cst = R(0);
+        const bool bb = (mk & M_BB) != 0;
+        if constexpr (SCALAR) {
+            R s = R(0);
+            sfor<Q>([&](auto I) { s += gg[I]; });
+            if (P.s_ads && bb) {
+                q = ((const R*)P.qads)[g.cell];
+                cst = ((const R*)P.cprev)[g.cell];
+            }
+            R src;
+            if (scalar_source<R>(P, bb, cst, q, !P.observe, src)) s += R(0.5) * src;
+            cval = s;
+        }
+
+        if (P.observe) {
+            P.obs_rho[g.cell] = double(rho);
+            sfor<D>([&](auto A) { P.obs_u[g.cell * D + A] = double(u[A]); });
+            if constexpr (SCALAR) P.obs_c[g.cell] = double(cval);
+        } else {
+            // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
+            if (P.residual) {
+                const R* mp = (const R*)P.mom_prev;
+                const double dr = double(rho) - double(mp[g.cell]);
+                racc[0] = dr * dr;
+                sfor<D>([&](auto A) {
+                    const double du = double(u[A]) - double(mp[(1 + A) * P.N + g.cell]);
+                    racc[1 + A] = du * du;
+                });
+                if constexpr (SCALAR) {
+                    const double dc = double(cval) - double(mp[(1 + D) * P.N + g.cell]);
+                    racc[4] = dc * dc;
+                }
+            }
+            if (P.write_mom) {
+                R* mc = (R*)P.mom_cur;
+                mc[g.cell] = rho;
+                sfor<D>([&](auto A) { mc[(1 + A) * P.N + g.cell] = u[A]; });
+                if constexpr (SCALAR) mc[(1 + D) * P.N + g.cell] = cval;
+            }
+            // ---- previous-step layers next to faces (anti-BB, extrapolation) ---------
+            if constexpr (FACEBC) {
+                if (P.any_face) {
+                    sfor<L::NF>([&](auto FF) {
+                        constexpr int Fc = FF;
+                        if (P.pb_dst[Fc]) {
+                            const int dist = face_dist(g, Fc, P);
+                            if (dist <= 1) {
+                                R* pb = (R*)P.pb_dst[Fc];
+                                const long long pl = P.pb_plane[Fc], pos = face_pos(g, Fc, P);
+                                sfor<D>([&](auto A) { pb[(dist * (D + 1) + A) * pl + pos] = u[A]; });
+                                pb[(dist * (D + 1) + D) * pl + pos] = cval;
+                            }
+                        }
+                    });
+                }
+            }
+
+            // ---- equilibrium + collision --------------------------------------------
+            R uu = R(0);
+            sfor<D>([&](auto A) { uu += u[A] * u[A]; });
+            R fe[Q];
+            sfor<Q>([&](auto I) { fe[I] = feq_i<L, R>(I, rho, u, uu); });
+            collide<VS, COLL, R>(P, f, fe, rho, u, F, force, P.tau, P.omega, P.op, P.om, P.rates, P.compat);
+            sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, f[I], R(L::w(I))); });
+
+            if constexpr (SCALAR) {
+                // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
+                R ge[Q];
+                sfor<Q>([&](auto I) { ge[I] = feq_i<L, R>(I, cval, u, uu); });
+                if (P.s_coll == COLL_BGK) {
+                    const R w1 = R(P.s_omega), w0 = R(1) - R(P.s_omega);
+                    R src;
+                    const bool has = scalar_source<R>(P, bb, cval, q, true, src);
+                    const R cb = R(1.0 - 0.5 / P.s_tau);
+                    sfor<Q>([&](auto I) {
+                        R v = w0 * gg[I] + w1 * ge[I];
+                        if (has) v += cb * R(L::w(I)) * src;
+                        gg[I] = v;
+                    });
+                } else {   // TRT, no source (src/lib.rs:118-127)
+                    const R wp = R(P.s_op), wm = R(P.s_om);
+                    R out[Q];
+                    sfor<Q>([&](auto I) {
+                        constexpr int i = I, ib = L::qbar(i);
+                        out[i] = gg[i] - wp * (R(0.5) * (gg[i] + gg[ib]) - R(0.5) * (ge[i] + ge[ib])) -
+                                 wm * (R(0.5) * (gg[i] - gg[ib]) - R(0.5) * (ge[i] - ge[ib]));
+                    });
+                    sfor<Q>([&](auto I) { gg[I] = out[I]; });
+                }
+                sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = gg[I]; });
+                if (P.s_ads && bb) {
+                    ((R*)P.qads)[g.cell] = q;
+                    ((R*)P.cprev)[g.cell] = cval;
+                }
+            }
+        }
+    }
+    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+}
+
+}  // namespace lbf

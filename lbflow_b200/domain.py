@@ -1,0 +1,170 @@
+"""`Domain`: one lattice on the GPU, driven through the C ABI of include/lbflow.h.
+
+This replaces the reference's momentum::Lattice (+ passive_scalar::Lattice)
+object graph: it is created from the same Parameters values, keeps the
+populations resident on the device, and exposes the reference's passes as
+calls (init / step / run / residuals / moments).  There is no CPU fallback:
+creating a Domain loads liblbflow_b200.so or raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _abi
+from . import momentum as _m
+from . import passive_scalar as _ps
+from .core import VelocitySet
+
+
+def _ptr(a: Optional[np.ndarray], ctype=C.c_double):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _stream_handle(stream) -> Optional[int]:
+    """Accept None, an int handle, or a torch.cuda.Stream."""
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+class Domain:
+    def __init__(self, params: _m.Parameters, scalar: Optional[_ps.Parameters] = None,
+                 desc: Optional[_abi.DomainDesc] = None, scalar_desc: Optional[_abi.ScalarDesc] = None):
+        self.lib = _abi.load()
+        keep = []
+        if desc is None:
+            desc, keep = _m.to_desc(params)
+        self.desc = desc
+        vs = VelocitySet(desc.velocity_set)
+        self.d, self.q = vs.d, vs.q
+        self.n = tuple(int(desc.n[a]) for a in range(self.d))
+        self.N = int(np.prod(self.n))
+        h = C.c_void_p()
+        _abi.check(self.lib.lbf_domain_create(C.byref(desc), C.byref(h)))
+        self.h = h
+        self.has_scalar = False
+        self.scalar_name = None
+        try:
+            if scalar is not None or scalar_desc is not None:
+                if scalar_desc is None:
+                    scalar_desc, k2 = _ps.to_desc(scalar, self.n)
+                    keep += k2
+                    self.scalar_name = scalar.scalar_name
+                _abi.check(self.lib.lbf_scalar_attach(self.h, C.byref(scalar_desc)))
+                self.has_scalar = True
+        except Exception:
+            self.close()
+            raise
+        self._keep = keep   # the library copied them; kept only until here
+
+    # -- lifecycle -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lbf_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- passes ---------------------------------------------------------------
+    def init(self, stream=None) -> "Domain":
+        _abi.check(self.lib.lbf_domain_init(self.h, _stream_handle(stream)))
+        return self
+
+    def step(self, n: int = 1, residual_interval: int = 0, stream=None) -> "Domain":
+        _abi.check(self.lib.lbf_domain_step(self.h, int(n), int(residual_interval), _stream_handle(stream)))
+        return self
+
+    def run(self, max_iterations: int, residual_interval: int = 1, tol_density: float = 1e-7,
+            tol_velocity: float = 1e-7, tol_scalar: float = 1e-7, stream=None) -> int:
+        steps = C.c_int64()
+        _abi.check(self.lib.lbf_domain_run(self.h, int(max_iterations), int(residual_interval), tol_density,
+                                           tol_velocity, tol_scalar, C.byref(steps), _stream_handle(stream)))
+        return steps.value
+
+    @property
+    def time_step(self) -> int:
+        t = C.c_int64()
+        _abi.check(self.lib.lbf_domain_time_step(self.h, C.byref(t)))
+        return t.value
+
+    @property
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        _abi.check(self.lib.lbf_domain_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def residuals(self):
+        out = np.zeros(8)
+        t = C.c_int64()
+        _abi.check(self.lib.lbf_domain_residuals(self.h, _ptr(out), C.byref(t)))
+        return out[: 1 + self.d + (1 if self.has_scalar else 0)], t.value
+
+    def moments(self, stream=None):
+        """(density[N], velocity[N, D], scalar[N] or None) at the current time step."""
+        rho = np.zeros(self.N)
+        u = np.zeros(self.N * self.d)
+        c = np.zeros(self.N) if self.has_scalar else None
+        _abi.check(self.lib.lbf_domain_get_moments(self.h, _ptr(rho), _ptr(u), _ptr(c), _stream_handle(stream)))
+        return rho, u.reshape(self.N, self.d), c
+
+    def q_ads(self):
+        out = np.zeros(self.N)
+        _abi.check(self.lib.lbf_domain_get_q_ads(self.h, _ptr(out)))
+        return out
+
+    def inventory(self, stream=None):
+        out = np.zeros(8)
+        _abi.check(self.lib.lbf_domain_inventory(self.h, _ptr(out), _stream_handle(stream)))
+        return out[: 3 + self.d]
+
+    def node_class(self):
+        cls = np.zeros(self.N, np.uint32)
+        links = np.zeros(self.N, np.uint32)
+        _abi.check(self.lib.lbf_domain_get_node_class(self.h, _ptr(cls, C.c_uint32), _ptr(links, C.c_uint32)))
+        return cls, links
+
+
+def tables(vs: int) -> dict:
+    """Velocity-set tables as compiled into the device code (lbf_velocity_set_tables)."""
+    lib = _abi.load()
+    d, q = C.c_int32(), C.c_int32()
+    c = np.zeros(81, np.int32); w = np.zeros(27); qb = np.zeros(27, np.int32)
+    qf = np.zeros(54, np.int32); nrm = np.zeros(6, np.int32); M = np.zeros(729); Mi = np.zeros(729)
+    i32 = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))  # noqa: E731
+    _abi.check(lib.lbf_velocity_set_tables(vs, C.byref(d), C.byref(q), i32(c), _ptr(w), i32(qb), i32(qf), i32(nrm),
+                                           _ptr(M), _ptr(Mi)))
+    q = q.value
+    return {"d": d.value, "q": q, "c": c[:3 * q].reshape(q, 3), "w": w[:q], "q_bar": qb[:q],
+            "q_faces": qf.reshape(6, 9), "face_normal": nrm, "mrt": M[:q * q].reshape(q, q),
+            "mrt_inverse": Mi[:q * q].reshape(q, q)}
+
+
+def solve_arrays(params: _m.Parameters, nsteps: int, scalar: Optional[_ps.Parameters] = None, stream=None):
+    """lbf_solve: one call with host buffers (create, init, nsteps main_steps, moments)."""
+    lib = _abi.load()
+    desc, keep = _m.to_desc(params)
+    vs = VelocitySet(desc.velocity_set)
+    N = int(np.prod([desc.n[a] for a in range(vs.d)]))
+    sdesc = None
+    if scalar is not None:
+        sdesc, k2 = _ps.to_desc(scalar, [desc.n[a] for a in range(vs.d)])
+        keep += k2
+    rho = np.zeros(N); u = np.zeros(N * vs.d); c = np.zeros(N) if scalar is not None else None
+    _abi.check(lib.lbf_solve(C.byref(desc), C.byref(sdesc) if sdesc is not None else None, int(nsteps),
+                             _ptr(rho), _ptr(u), _ptr(c), _stream_handle(stream)))
+    return rho, u.reshape(N, vs.d), c
