@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block", type=int, default=0, help="override the x block size")
+    ap.add_argument("--no-stage", action="store_true", help="plain-load sweep instead of bulk-copy staging")
     return ap.parse_args()
 
 
@@ -204,7 +205,10 @@ def run_engine(args, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     dom = Domain(p)
     if args.block:
-        pass
+        dom.set_option(_abi.LBF_OPT_BLOCK_X, args.block)
+    if args.no_stage:
+        dom.set_option(_abi.LBF_OPT_STAGE, 0)
+    staged = bool(dom.get_option(_abi.LBF_OPT_STAGE))
     dom.init(stream)
     dom.step(args.warmup, 0, stream)
     torch.cuda.synchronize()
@@ -265,7 +269,8 @@ def run_engine(args, rank, world, local_rank):
             "data": "synthetic (seeded sphere packing)",
             "config": {"workload": workload_name(args), "storage": args.storage, "n_fluid": n_fluid,
                        "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "sweep": "bulk-copy staged" if staged else "plain loads"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},

@@ -208,6 +208,14 @@ lbf_status lbf_domain_inventory(lbf_domain* dom, double* out, void* stream);
 /* Node classes (LBF_CLASS_* bits) and solid-neighbour link masks (bit i: the
  * neighbour along c_i is solid), computed on the device. */
 lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint32_t* links);
+/* Launch options (no reference counterpart; used by the autotuner):
+ * LBF_OPT_BLOCK_X  threads per block along x for the unstaged sweep (0 = heuristic)
+ * LBF_OPT_STAGE    1 = stage the pull rows in shared memory with bulk copies when the
+ *                  shape allows it (nx <= 512, rows 16-byte aligned); 0 = plain loads.
+ * lbf_domain_get_option(LBF_OPT_STAGE) reports whether staging is in effect. */
+enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1 };
+lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
+lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */
 lbf_status lbf_domain_time_step(lbf_domain* dom, int64_t* t);
 /* Device bytes held by the domain. */

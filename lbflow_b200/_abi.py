@@ -24,6 +24,8 @@ LBF_INNER_ANTI_BOUNCE_BACK, LBF_INNER_BOUNCE_BACK = range(2)
 LBF_STORE_F64, LBF_STORE_F32, LBF_STORE_F16DEV, LBF_STORE_BF16DEV = range(4)
 LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 
+LBF_OPT_BLOCK_X, LBF_OPT_STAGE = range(2)
+
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2
 LBF_CLASS_FACE_SHIFT = 2
@@ -98,6 +100,8 @@ SIGNATURES = {
     "lbf_domain_inventory": (_I32, [_P, _PD, _P]),
     "lbf_domain_get_node_class": (_I32, [_P, _PU32, _PU32]),
     "lbf_domain_time_step": (_I32, [_P, _PI64]),
+    "lbf_domain_set_option": (_I32, [_P, _I32, _I64]),
+    "lbf_domain_get_option": (_I32, [_P, _I32, _PI64]),
     "lbf_domain_device_bytes": (_I32, [_P, _PI64]),
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),

@@ -141,7 +141,8 @@ def packed_bed_scalar(n: Sequence[int] = (192, 192, 384), porosity: float = 0.6,
     Inlet z = 0 (Bottom): Zou-He velocity u_z (engine extension) or, for the
     reference-expressible variant, a moving-wall BounceBack with the same
     velocity; scalar Dirichlet C = 1.  Outlet z = nz-1 (Top): AntiBounceBack
-    density 1; scalar zeroth-order outflow.  Side walls: NoSlip, scalar BBNoFlux.
+    density 1; scalar second-order extrapolation outflow (all populations).  Side
+    walls: NoSlip, scalar BBNoFlux.
     """
     if mask is None:
         mask = sphere_pack(n, porosity, rmin, rmax, seed)
@@ -156,7 +157,7 @@ def packed_bed_scalar(n: Sequence[int] = (192, 192, 384), porosity: float = 0.6,
                        initial_scalar_value=ps.InitialScalarValue.Uniform(0.0), velocity_set=VelocitySet.D3Q19,
                        boundary_conditions=[(W, ps.BBNoFlux), (E, ps.BBNoFlux), (S, ps.BBNoFlux),
                                             (N, ps.BBNoFlux), (B, ps.AntiBounceBack(1.0)),
-                                            (T, ps.AntiBBNoFlux)],
+                                            (T, ps.SecondOrderNoFlux(unknown_populations_only=False))],
                        inner_boundary_condition=ps.InnerBounceBack,
                        adsorption_parameters=ps.AdsorptionParameters(ps.Langmuir(ka, kd, q_max), 0.0))
     return mp, sp

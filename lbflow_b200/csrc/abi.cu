@@ -141,6 +141,8 @@ struct lbf_domain {
     uint8_t* dtype = nullptr;
     void* mom[2] = {nullptr, nullptr};
     void* pb[6][2] = {};
+    void* snap[6] = {};
+    unsigned outflow = 0;   // faces with a scalar extrapolation outflow (face pass)
     long long pb_plane[6] = {0, 0, 0, 0, 0, 0};
     void* qads = nullptr;
     void* cprev = nullptr;
@@ -154,6 +156,8 @@ struct lbf_domain {
     long long t = 0;
     long long res_step = -1;
     int block_x = 0;
+    bool stage = true;            // use the bulk-copy staged sweep when the shape allows it
+    int* err = nullptr;           // device flag: a bounded wait gave up
     cudaStream_t last_stream = nullptr;
     long long bytes = 0;
 
@@ -162,8 +166,9 @@ struct lbf_domain {
             cudaFree(pop[k]); cudaFree(gpop[k]); cudaFree(mom[k]);
             for (int f = 0; f < 6; ++f) cudaFree(pb[f][k]);
         }
+        for (int f = 0; f < 6; ++f) cudaFree(snap[f]);
         cudaFree(mask); cudaFree(dtype); cudaFree(qads); cudaFree(cprev); cudaFree(c_init_dev);
-        cudaFree(accum); cudaFree(res_dev); cudaFree(obs); cudaFree(counts);
+        cudaFree(accum); cudaFree(res_dev); cudaFree(obs); cudaFree(counts); cudaFree(err);
         if (res_host) cudaFreeHost(res_host);
     }
     int nfields() const { return 1 + d + (scalar ? 1 : 0); }
@@ -305,7 +310,7 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     SetupParams S{};
     S.nx = (int)D->n[0]; S.ny = (int)D->n[1]; S.nz = (int)D->n[2]; S.N = N;
     S.type = D->dtype; S.cls = cls; S.links = links; S.mask = D->mask;
-    S.fold_faces = fold; S.explicit_faces = expl; S.skip_faces = 0; S.counts = D->counts;
+    S.fold_faces = fold; S.explicit_faces = expl; S.skip_faces = D->outflow; S.counts = D->counts;
     Launch L{dim3((unsigned)((N + 255) / 256)), dim3(256), s};
     if (e == cudaSuccess) {
         e = D->vs == LBF_D2Q9 ? launch_setup<VS_D2Q9>(S, L)
@@ -321,14 +326,18 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("node classification: ") + cudaGetErrorString(e));
     D->n_fluid = cnt[0];
     D->n_bb = cnt[1];
-    // face layers
+    // face layers and outflow snapshots
+    for (int f = 0; f < D->nfaces; ++f) D->pb_plane[f] = N / D->n[f / 2];
     for (int f = 0; f < 6; ++f) {
-        if (!face_needs_layers(D, f)) continue;
-        const int ax = f / 2;
-        const long long plane = N / D->n[ax];
-        D->pb_plane[f] = plane;
-        for (int k = 0; k < 2; ++k)
-            if (!D->pb[f][k] && (st = dmalloc(D, &D->pb[f][k], 2 * (D->d + 1) * plane * rt_bytes(D->st)))) return st;
+        const long long plane = D->pb_plane[f];
+        if (face_needs_layers(D, f))
+            for (int k = 0; k < 2; ++k)
+                if (!D->pb[f][k] && (st = dmalloc(D, &D->pb[f][k], 2 * (D->d + 1) * plane * rt_bytes(D->st)))) return st;
+        if ((D->outflow >> f & 1u) && !D->snap[f]) {
+            const size_t b = 2 * (size_t)D->q * plane * rt_bytes(D->st);
+            if ((st = dmalloc(D, &D->snap[f], b))) return st;
+            CK(cudaMemsetAsync(D->snap[f], 0, b, s));   // solid neighbours read as zero populations
+        }
     }
     D->prepared = true;
     return LBF_OK;
@@ -339,6 +348,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.nx = (int)D->n[0]; P.ny = (int)D->n[1]; P.nz = (int)D->n[2]; P.dims = D->d;
     P.N = D->N;
     P.mask = D->mask;
+    P.err = D->err;
     const size_t eb = st_bytes(D->st);
     for (int i = 0; i < D->q; ++i) {
         P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->N * eb;
@@ -356,6 +366,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
         P.pb_dst[f] = D->pb[f][t & 1];
         if (D->pb[f][0]) P.any_face = 1;
     }
+    for (int f = 0; f < 6; ++f) P.snap[f] = D->snap[f];
     P.mom_prev = D->mom[(t + 1) & 1];
     P.mom_cur = D->mom[t & 1];
     P.accum = D->accum;
@@ -379,15 +390,45 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     }
 }
 
-cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
-    const dim3 b = step_block(D);
-    Launch L{step_grid(D, b), b, s};
+cudaError_t launch_one(lbf_domain* D, const StepParams& P, bool stage, const Launch& L) {
     const int coll = D->desc.collision.kind;
     switch (D->vs) {
-        case LBF_D2Q9: return launch_step<VS_D2Q9>(coll, D->st, D->facebc, D->scalar, P, nullptr, L);
-        case LBF_D3Q19: return launch_step<VS_D3Q19>(coll, D->st, D->facebc, D->scalar, P, nullptr, L);
-        default: return launch_step<VS_D3Q27>(coll, D->st, D->facebc, D->scalar, P, D->lam.data(), L);
+        case LBF_D2Q9: return launch_step<VS_D2Q9>(coll, D->st, D->facebc, D->scalar, stage, P, nullptr, L);
+        case LBF_D3Q19: return launch_step<VS_D3Q19>(coll, D->st, D->facebc, D->scalar, stage, P, nullptr, L);
+        default: return launch_step<VS_D3Q27>(coll, D->st, D->facebc, D->scalar, stage, P, D->lam.data(), L);
     }
+}
+
+// Whether the staged (bulk-copy) sweep applies: one block per x-row, rows
+// 16-byte aligned, the staged rows fit in shared memory.
+bool can_stage(const lbf_domain* D) {
+    const size_t tb = st_bytes(D->st), rb = rt_bytes(D->st);
+    if (D->n[0] > 512 || (D->n[0] * tb) % 16 != 0) return false;
+    if (D->scalar && (D->n[0] * rb) % 16 != 0) return false;
+    return stage_smem(D->q, D->n[0], tb, rb, D->scalar) <= 200 * 1024;
+}
+
+// The bulk sweep, then one face pass per scalar outflow face.
+cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    const bool stage = D->stage && can_stage(D);
+    const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
+    cudaError_t e = launch_one(D, P, stage, Launch{step_grid(D, b), b, s});
+    for (int f = 0; f < D->nfaces && e == cudaSuccess; ++f) {
+        if (!(D->outflow >> f & 1u)) continue;
+        StepParams F = P;
+        F.face_pass = 1;
+        F.fp_face = f;
+        e = launch_one(D, F, false, Launch{dim3((unsigned)((D->pb_plane[f] + 127) / 128)), dim3(128), s});
+    }
+    return e;
+}
+
+// Reads the device error flag after a synchronisation point.
+lbf_status check_err(lbf_domain* D) {
+    int h = 0;
+    CK(cudaMemcpy(&h, D->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) return fail(LBF_ETIMEOUT, "a bounded wait in the step kernel gave up (staged copy did not complete)");
+    return LBF_OK;
 }
 
 lbf_status ensure_mom(lbf_domain* D) {
@@ -571,6 +612,8 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
         if ((st = dmalloc(D, &D->pop[k], pbytes))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->accum, NSLOT * NACC * sizeof(double)))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->res_dev, 8 * sizeof(double)))) { delete D; return st; }
+    if ((st = dmalloc(D, (void**)&D->err, sizeof(int)))) { delete D; return st; }
+    if (cudaMemset(D->err, 0, sizeof(int)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
     if (cudaMallocHost(&D->res_host, 8 * sizeof(double)) != cudaSuccess) { delete D; return fail(LBF_ENOMEM, "pinned alloc"); }
     std::memset(D->res_host, 0, 8 * sizeof(double));
     if (cudaMemset(D->accum, 0, NSLOT * NACC * sizeof(double)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
@@ -591,9 +634,19 @@ lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
     for (int f = 0; f < D->nfaces; ++f) {
         const int k = s->bc[f].kind;
         if (k < LBF_SBC_ANTI_BOUNCE_BACK || k > LBF_SBC_PERIODIC) return fail(LBF_EINVAL, "bad scalar BC kind");
-        if (k == LBF_SBC_ZEROTH_ORDER_NO_FLUX || k == LBF_SBC_SECOND_ORDER_NO_FLUX)
-            return fail(LBF_EUNSUPPORTED, "extrapolation outflow for the scalar is not built on the device yet");
     }
+    unsigned outflow = 0;
+    for (int f = 0; f < D->nfaces; ++f) {
+        const int k = s->bc[f].kind;
+        if (k != LBF_SBC_ZEROTH_ORDER_NO_FLUX && k != LBF_SBC_SECOND_ORDER_NO_FLUX) continue;
+        if (D->n[f / 2] < 4) return fail(LBF_EINVAL, "an extrapolation outflow face needs >= 4 nodes along its normal");
+        outflow |= 1u << f;
+    }
+    for (int f = 0; f < D->nfaces; ++f)
+        for (int g = 0; g < D->nfaces; ++g)
+            if ((outflow >> f & 1u) && (outflow >> g & 1u) && f / 2 != g / 2)
+                return fail(LBF_EUNSUPPORTED, "extrapolation outflow on two faces that share an edge is not built");
+    D->outflow = outflow;
     D->sdesc = *s;
     D->sdesc.initial_scalar_field = nullptr;
     if (s->initial_scalar_field) D->c0.assign(s->initial_scalar_field, s->initial_scalar_field + D->N);
@@ -652,6 +705,8 @@ lbf_status lbf_domain_run(lbf_domain* D, int64_t max_iterations, int64_t k, doub
 lbf_status lbf_domain_residuals(lbf_domain* D, double* out, int64_t* time_step) {
     if (!D || !out) return fail(LBF_EINVAL, "null argument");
     CK(cudaStreamSynchronize(D->last_stream));
+    lbf_status est = check_err(D);
+    if (est) return est;
     for (int k = 0; k < D->nfields(); ++k) out[k] = D->res_host[k];
     if (D->scalar && D->d == 2) out[3] = D->res_host[4];
     if (time_step) *time_step = D->res_step;
@@ -668,6 +723,7 @@ lbf_status lbf_domain_get_moments(lbf_domain* D, double* rho, double* u, double*
     if (u) CK(cudaMemcpyAsync(u, D->obs + N, N * D->d * 8, cudaMemcpyDeviceToHost, s));
     if (c && D->scalar) CK(cudaMemcpyAsync(c, D->obs + N * (1 + D->d), N * 8, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if ((st = check_err(D))) return st;
     // solid nodes keep their initial values (they are never updated)
     for (long long i = 0; i < N; ++i) {
         if (!D->type[i]) continue;
@@ -738,6 +794,30 @@ lbf_status lbf_domain_device_bytes(lbf_domain* D, int64_t* b) {
     if (!D || !b) return fail(LBF_EINVAL, "null argument");
     *b = D->bytes;
     return LBF_OK;
+}
+
+lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
+    if (!D) return fail(LBF_EINVAL, "null domain");
+    switch (option) {
+        case LBF_OPT_BLOCK_X:
+            if (value < 0 || value > 1024 || (value % 32)) return fail(LBF_EINVAL, "block_x must be 0 or a multiple of 32 <= 1024");
+            D->block_x = (int)value;
+            return LBF_OK;
+        case LBF_OPT_STAGE:
+            D->stage = value != 0;
+            return LBF_OK;
+        default:
+            return fail(LBF_EINVAL, "unknown option");
+    }
+}
+
+lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) {
+    if (!D || !value) return fail(LBF_EINVAL, "null argument");
+    switch (option) {
+        case LBF_OPT_BLOCK_X: *value = D->block_x; return LBF_OK;
+        case LBF_OPT_STAGE: *value = (D->stage && can_stage(D)) ? 1 : 0; return LBF_OK;
+        default: return fail(LBF_EINVAL, "unknown option");
+    }
 }
 
 lbf_status lbf_domain_destroy(lbf_domain* D) {

@@ -62,6 +62,9 @@ __global__ void k_setup(const SetupParams S) {
             if (S.skip_faces >> F & 1u) mask |= M_SKIP;
         }
     });
+    const int dist[6] = {x, S.nx - 1 - x, y, S.ny - 1 - y, z, S.nz - 1 - z};
+    for (int F = 0; F < L::NF; ++F)
+        if ((S.skip_faces >> F & 1u) && (dist[F] == 1 || dist[F] == 2)) mask |= M_NEAR;
     S.cls[cell] = cls;
     S.links[cell] = links;
     S.mask[cell] = mask;
@@ -109,8 +112,9 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
     if (fluid) {
         sfor<Q>([&](auto Ii) {
             constexpr int i = Ii;
-            const double fe = feq_i<L, double>(i, rho, u, uu);
-            S::st(const_cast<void*>(P.srcp[i]), cell, R(fe), R(L::w(i)));
+            // FP32-compute formats store h = f_eq - w (evaluated in FP64)
+            const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
+            S::st(const_cast<void*>(P.srcp[i]), cell, R(fe));
         });
         if constexpr (SCALAR) {
             sfor<Q>([&](auto Ii) {

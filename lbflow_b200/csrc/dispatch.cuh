@@ -12,8 +12,12 @@ struct Launch {
 };
 
 template <int VS>
-cudaError_t launch_step(int coll, int st, bool facebc, bool scalar, const StepParams& base, const double* lam,
-                        const Launch& L);
+cudaError_t launch_step(int coll, int st, bool facebc, bool scalar, bool stage, const StepParams& base,
+                        const double* lam, const Launch& L);
+// Dynamic shared memory of the staged kernel: Q rows (+ Q scalar rows) + mbarrier.
+inline size_t stage_smem(int q, long long nx, size_t tbytes, size_t rbytes, bool scalar) {
+    return (size_t)q * nx * (tbytes + (scalar ? rbytes : 0)) + 16;
+}
 template <int VS>
 cudaError_t launch_init(int st, bool scalar, const StepParams& P, const InitParams& I, void* const* pb,
                         const Launch& L);
@@ -29,10 +33,23 @@ inline void fill_lam(KParams<VS_D3Q27>& kp, const double* lam) {
     }
 }
 
-#define LBF_STEP_CASE(C_, S_, FB_, SC_)                                                 \
-    if (coll == C_ && st == S_ && facebc == FB_ && scalar == SC_) {                      \
-        k_step<VS, C_, S_, FB_, SC_><<<L.grid, L.block, 0, L.stream>>>(kp);              \
-        return cudaGetLastError();                                                      \
+#define LBF_STEP_CASE(C_, S_, FB_, SC_)                                                                   \
+    if (coll == C_ && st == S_ && facebc == FB_ && scalar == SC_) {                                        \
+        if (stage) {                                                                                       \
+            const size_t sm = stage_smem(Lat<VS>::Q, kp.nx, sizeof(typename Store<S_>::T),                \
+                                         sizeof(typename Store<S_>::R), SC_);                              \
+            static size_t sm_set = 0;                                                                      \
+            if (sm > 48 * 1024 && sm > sm_set) {                                                           \
+                cudaError_t e_ = cudaFuncSetAttribute(k_step<VS, C_, S_, FB_, SC_, true>,                  \
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+                if (e_ != cudaSuccess) return e_;                                                          \
+                sm_set = sm;                                                                               \
+            }                                                                                              \
+            k_step<VS, C_, S_, FB_, SC_, true><<<L.grid, L.block, sm, L.stream>>>(kp);                     \
+        } else {                                                                                           \
+            k_step<VS, C_, S_, FB_, SC_, false><<<L.grid, L.block, 0, L.stream>>>(kp);                     \
+        }                                                                                                  \
+        return cudaGetLastError();                                                                         \
     }
 #define LBF_STEP_ST(C_, S_)            \
     LBF_STEP_CASE(C_, S_, false, false) \
@@ -41,18 +58,34 @@ inline void fill_lam(KParams<VS_D3Q27>& kp, const double* lam) {
     LBF_STEP_ST(C_, ST_F64) LBF_STEP_ST(C_, ST_F32) LBF_STEP_ST(C_, ST_F16) LBF_STEP_ST(C_, ST_BF16) \
     LBF_STEP_CASE(C_, ST_F64, true, true) LBF_STEP_CASE(C_, ST_F32, true, true)
 
-#define LBF_INSTANTIATE(VS_)                                                                           \
+// One translation unit per (velocity set, collision) instantiates the step kernels.
+template <int VS, int COLL>
+cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const StepParams& base, const double* lam,
+                          const Launch& L);
+
+#define LBF_INSTANTIATE_COLL(VS_, COLL_)                                                               \
     template <>                                                                                        \
-    cudaError_t launch_step<VS_>(int coll, int st, bool facebc, bool scalar, const StepParams& base,   \
-                                 const double* lam, const Launch& L) {                                 \
+    cudaError_t launch_step_c<VS_, COLL_>(int st, bool facebc, bool scalar, bool stage,                \
+                                          const StepParams& base, const double* lam, const Launch& L) { \
         constexpr int VS = VS_;                                                                        \
+        const int coll = COLL_;                                                                        \
         KParams<VS> kp;                                                                                \
         static_cast<StepParams&>(kp) = base;                                                           \
         fill_lam(kp, lam);                                                                             \
-        LBF_STEP_COLL(COLL_BGK)                                                                        \
-        LBF_STEP_COLL(COLL_TRT)                                                                        \
-        LBF_STEP_COLL(COLL_MRT)                                                                        \
+        LBF_STEP_COLL(COLL_)                                                                           \
         return cudaErrorInvalidValue;                                                                  \
+    }
+
+#define LBF_INSTANTIATE(VS_)                                                                           \
+    template <>                                                                                        \
+    cudaError_t launch_step<VS_>(int coll, int st, bool facebc, bool scalar, bool stage,               \
+                                 const StepParams& base, const double* lam, const Launch& L) {         \
+        switch (coll) {                                                                                \
+            case COLL_BGK: return launch_step_c<VS_, COLL_BGK>(st, facebc, scalar, stage, base, lam, L); \
+            case COLL_TRT: return launch_step_c<VS_, COLL_TRT>(st, facebc, scalar, stage, base, lam, L); \
+            case COLL_MRT: return launch_step_c<VS_, COLL_MRT>(st, facebc, scalar, stage, base, lam, L); \
+            default: return cudaErrorInvalidValue;                                                     \
+        }                                                                                              \
     }                                                                                                  \
     template <>                                                                                        \
     cudaError_t launch_init<VS_>(int st, bool scalar, const StepParams& P, const InitParams& I,        \

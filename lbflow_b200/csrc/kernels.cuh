@@ -37,12 +37,15 @@ constexpr int COMPAT_REFERENCE = 0, COMPAT_PHYSICS = 1;
 // Per-node mask word.  Bits 0..26: the neighbour along c_i is solid (or, on the
 // lean path, a no-slip wall); bit 27 solid node; bit 28 bounce-back node (has a
 // solid neighbour, drives adsorption); bit 29 node needs explicit face BCs;
-// bit 30 node is updated by the face pass, not by the bulk sweep.
+// bit 30 node is updated by the face pass, not by the bulk sweep; bit 31 node
+// lies one or two layers inside a scalar extrapolation-outflow face (its
+// post-stream scalar populations are snapshotted for that face).
 constexpr uint32_t M_LINKS = (1u << 27) - 1u;
 constexpr uint32_t M_SOLID = 1u << 27;
 constexpr uint32_t M_BB = 1u << 28;
 constexpr uint32_t M_FACE = 1u << 29;
 constexpr uint32_t M_SKIP = 1u << 30;
+constexpr uint32_t M_NEAR = 1u << 31;   // 1 or 2 layers inside a scalar outflow face
 
 constexpr int NSLOT = 256;   // partial-sum slots of the FP64 reductions
 constexpr int NACC = 8;      // accumulators per slot
@@ -81,6 +84,12 @@ struct StepParams {
     int order[6];
     int any_face;
     int observe, write_mom, residual;
+    int face_pass, fp_face;   // face pass: update the nodes of face fp_face only
+    int* err;                 // set to 1 when a bounded wait gives up
+    // post-stream scalar populations of layers 1 and 2 inside each outflow face,
+    // written by the bulk sweep and read by the face pass of the same step:
+    // [layer 0/1][direction][plane node], compute type
+    void* snap[6];
     // previous-step moments of the two node layers next to each face:
     // [layer 0/1][field u_0..u_{D-1}, C][plane node], compute type
     const void* pb_src[6];
@@ -117,44 +126,47 @@ struct KParams<VS_D3Q27> : StepParams {
 };
 
 // ---- storage formats -----------------------------------------------------
+// FP64 storage holds the populations f_i themselves (the reference arithmetic).
+// The FP32-compute formats hold the deviation h_i = f_i - w_i ("DDF shifting"):
+// at low Mach numbers f_i ~ w_i, so storing and colliding h_i keeps the small
+// physical signal instead of rounding it against w_i.
 template <int ST>
 struct Store;
 template <>
 struct Store<ST_F64> {
     using T = double;
     using R = double;
-    __device__ static __forceinline__ R ld(const void* p, long long o, R) { return ((const T*)p)[o]; }
-    __device__ static __forceinline__ void st(void* p, long long o, R v, R) { ((T*)p)[o] = v; }
+    static constexpr bool DEV = false;
+    __device__ static __forceinline__ R ld(const void* p, long long o) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ R cvt(T v) { return v; }
+    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = v; }
 };
 template <>
 struct Store<ST_F32> {
     using T = float;
     using R = float;
-    __device__ static __forceinline__ R ld(const void* p, long long o, R) { return ((const T*)p)[o]; }
-    __device__ static __forceinline__ void st(void* p, long long o, R v, R) { ((T*)p)[o] = v; }
+    static constexpr bool DEV = true;
+    __device__ static __forceinline__ R ld(const void* p, long long o) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ R cvt(T v) { return v; }
+    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = v; }
 };
-// 16-bit deviation formats: the stored value is f_i - w_i.
 template <>
 struct Store<ST_F16> {
     using T = __half;
     using R = float;
-    __device__ static __forceinline__ R ld(const void* p, long long o, R w) {
-        return __half2float(((const T*)p)[o]) + w;
-    }
-    __device__ static __forceinline__ void st(void* p, long long o, R v, R w) {
-        ((T*)p)[o] = __float2half_rn(v - w);
-    }
+    static constexpr bool DEV = true;
+    __device__ static __forceinline__ R ld(const void* p, long long o) { return __half2float(((const T*)p)[o]); }
+    __device__ static __forceinline__ R cvt(T v) { return __half2float(v); }
+    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = __float2half_rn(v); }
 };
 template <>
 struct Store<ST_BF16> {
     using T = __nv_bfloat16;
     using R = float;
-    __device__ static __forceinline__ R ld(const void* p, long long o, R w) {
-        return __bfloat162float(((const T*)p)[o]) + w;
-    }
-    __device__ static __forceinline__ void st(void* p, long long o, R v, R w) {
-        ((T*)p)[o] = __float2bfloat16_rn(v - w);
-    }
+    static constexpr bool DEV = true;
+    __device__ static __forceinline__ R ld(const void* p, long long o) { return __bfloat162float(((const T*)p)[o]); }
+    __device__ static __forceinline__ R cvt(T v) { return __bfloat162float(v); }
+    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = __float2bfloat16_rn(v); }
 };
 
 // ---- node geometry -----------------------------------------------------------
@@ -232,6 +244,20 @@ __device__ __forceinline__ R feq_i(int i, R rho, const R* u, R uu) {
     for (int a = 0; a < L::D; ++a) cu += u[a] * R(L::c(i, a));
     return R(L::w(i)) * rho * (R(1) + cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
 }
+// f_eq - w_i = w_i (drho + rho (3 c.u + 4.5 (c.u)^2 - 1.5 u.u)), drho = rho - 1.
+template <class L, class R>
+__device__ __forceinline__ R heq_i(int i, R rho, R drho, const R* u, R uu) {
+    R cu = R(0);
+#pragma unroll
+    for (int a = 0; a < L::D; ++a) cu += u[a] * R(L::c(i, a));
+    return R(L::w(i)) * (drho + rho * (cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3)));
+}
+// Equilibrium in the register representation of the storage format.
+template <class L, bool DEV, class R>
+__device__ __forceinline__ R eq_i(int i, R rho, R drho, const R* u, R uu) {
+    if constexpr (DEV) return heq_i<L, R>(i, rho, drho, u, uu);
+    else return feq_i<L, R>(i, rho, u, uu);
+}
 
 // Guo source without the (1 - omega/2) factor (src/kernel.rs:122-154).
 template <class L, class R>
@@ -247,13 +273,16 @@ __device__ __forceinline__ R guo_i(int i, const R* u, const R* F) {
 
 // Reference MRT equilibrium moments, bug for bug
 // (src/velocity_set/d2q9.rs:247-264, src/velocity_set/d3q19.rs:550-587).
-template <int VS, class R>
-__device__ __forceinline__ void meq_reference(R rho, const R* u, R* m) {
+// With DEV the moments of the weights (M w: [1,-2,1,0..] for D2Q9,
+// [1,-11,3,0..] for D3Q19) are subtracted, as the populations are h = f - w.
+template <int VS, bool DEV, class R>
+__device__ __forceinline__ void meq_reference(R rho, R drho, const R* u, R* m) {
+    const R base = DEV ? drho : rho;
     if constexpr (VS == VS_D2Q9) {
         const R s = u[0] * u[0] + u[1] * u[1];
-        m[0] = rho;
-        m[1] = rho - R(3) * rho * s;
-        m[2] = R(9) * rho * u[0] * u[0] * u[1] * u[1] - R(3) * rho * s + rho;
+        m[0] = base;
+        m[1] = DEV ? (drho + R(3)) - R(3) * rho * s : rho - R(3) * rho * s;
+        m[2] = R(9) * rho * u[0] * u[0] * u[1] * u[1] - R(3) * rho * s + base;
         m[3] = rho * u[0];
         m[4] = R(3) * rho * u[0] * u[0] * u[0] - rho * u[0];
         m[5] = rho * u[1];
@@ -263,9 +292,9 @@ __device__ __forceinline__ void meq_reference(R rho, const R* u, R* m) {
     } else if constexpr (VS == VS_D3Q19) {
         const R s = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
         const R bug = R(2) * rho * u[0] * u[0] - rho * (u[1] * u[1] + u[2] + u[2]);
-        m[0] = rho;
-        m[1] = R(-11) * rho + R(19) * rho * s;
-        m[2] = R(3) * rho - R(5.5) * rho * s;
+        m[0] = base;
+        m[1] = R(-11) * base + R(19) * rho * s;
+        m[2] = R(3) * base - R(5.5) * rho * s;
         m[3] = rho * u[0];
         m[4] = R(-2.0 / 3.0) * rho * u[0];
         m[5] = rho * u[1];
@@ -297,9 +326,9 @@ __device__ __forceinline__ R lam_at(const KParams<VS>& P, int k) {
 
 // Collision in place on f (registers) given feq; src/kernel.rs:28-120 and the
 // force source of src/momentum/node.rs:311-333 (BGK) / the physics mode.
-template <int VS, int COLL, class R>
+template <int VS, int COLL, bool DEV, class R>
 __device__ __forceinline__ void collide(const KParams<VS>& P, R (&f)[Lat<VS>::Q], const R (&fe)[Lat<VS>::Q], R rho,
-                                        const R* u, const R* F, bool force, double tau, double omega,
+                                        R drho, const R* u, const R* F, bool force, double tau, double omega,
                                         double op, double om, const double* rates, int compat) {
     using L = Lat<VS>;
     constexpr int Q = L::Q;
@@ -358,7 +387,7 @@ __device__ __forceinline__ void collide(const KParams<VS>& P, R (&f)[Lat<VS>::Q]
                 m[k] = a;
             });
             if (compat == COMPAT_REFERENCE) {
-                meq_reference<VS, R>(rho, u, me);
+                meq_reference<VS, DEV, R>(rho, drho, u, me);
             } else {
                 sfor<Q>([&](auto K) {
                     constexpr int k = K;
@@ -403,39 +432,41 @@ __device__ __forceinline__ void collide(const KParams<VS>& P, R (&f)[Lat<VS>::Q]
 }
 
 // D2Q9 Zou-He, src/velocity_set/d2q9.rs:165-245 (formulas verbatim).
+// `one` is 1 when f holds deviations h = f - w (the weights of the known
+// populations in each sum add up to 1), 0 otherwise.
 template <class R>
-__device__ __forceinline__ void zou_he_d2q9(int face, R* f, const FaceBC& b) {
+__device__ __forceinline__ void zou_he_d2q9(int face, R* f, const FaceBC& b, R one) {
     const bool vel = !b.has_rho;
     R rho, ux, uy;
     switch (face) {
         case 0:
             uy = R(b.u[1]);
-            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) - ux) * (f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
-            else { rho = R(b.rho); ux = R(1) - R(1) / rho * (f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
+            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) - ux) * (one + f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
+            else { rho = R(b.rho); ux = R(1) - R(1) / rho * (one + f[0] + f[2] + f[4] + R(2) * (f[3] + f[6] + f[7])); }
             f[1] = f[3] + R(2.0 / 3.0) * rho * ux;
             f[5] = f[7] - R(0.5) * (f[2] - f[4]) + R(0.5) * rho * uy + R(1.0 / 6.0) * rho * ux;
             f[8] = f[6] + R(0.5) * (f[2] - f[4]) - R(0.5) * rho * uy + R(1.0 / 6.0) * rho * ux;
             break;
         case 1:
             uy = R(b.u[1]);
-            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) + ux) * (f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])); }
-            else { rho = R(b.rho); ux = R(1) / rho * (f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])) - R(1); }
+            if (vel) { ux = R(b.u[0]); rho = R(1) / (R(1) + ux) * (one + f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])); }
+            else { rho = R(b.rho); ux = R(1) / rho * (one + f[0] + f[2] + f[4] + R(2) * (f[1] + f[5] + f[8])) - R(1); }
             f[3] = f[1] - R(2.0 / 3.0) * rho * ux;
             f[7] = f[5] + R(0.5) * (f[2] - f[4]) - R(0.5) * rho * uy - R(1.0 / 6.0) * rho * ux;
             f[6] = f[8] - R(0.5) * (f[2] - f[4]) + R(0.5) * rho * uy - R(1.0 / 6.0) * rho * ux;
             break;
         case 2:
             ux = R(b.u[0]);
-            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) - uy) * (f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
-            else { rho = R(b.rho); uy = R(1) - R(1) / rho * (f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
+            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) - uy) * (one + f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
+            else { rho = R(b.rho); uy = R(1) - R(1) / rho * (one + f[0] + f[1] + f[3] + R(2) * (f[4] + f[7] + f[8])); }
             f[2] = f[4] + R(2.0 / 3.0) * rho * uy;
             f[5] = f[7] - R(0.5) * (f[1] - f[3]) + R(0.5) * rho * ux + R(1.0 / 6.0) * rho * uy;
             f[6] = f[8] + R(0.5) * (f[1] - f[3]) - R(0.5) * rho * ux + R(1.0 / 6.0) * rho * uy;
             break;
         default:
             ux = R(b.u[0]);
-            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) + uy) * (f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])); }
-            else { rho = R(b.rho); uy = R(1) / rho * (f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])) - R(1); }
+            if (vel) { uy = R(b.u[1]); rho = R(1) / (R(1) + uy) * (one + f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])); }
+            else { rho = R(b.rho); uy = R(1) / rho * (one + f[0] + f[1] + f[3] + R(2) * (f[2] + f[5] + f[6])) - R(1); }
             f[4] = f[2] - R(2.0 / 3.0) * rho * uy;
             f[7] = f[5] + R(0.5) * (f[1] - f[3]) - R(0.5) * rho * ux - R(1.0 / 6.0) * rho * uy;
             f[8] = f[6] - R(0.5) * (f[1] - f[3]) + R(0.5) * rho * ux - R(1.0 / 6.0) * rho * uy;
@@ -445,10 +476,10 @@ __device__ __forceinline__ void zou_he_d2q9(int face, R* f, const FaceBC& b) {
 
 // D3Q19 Zou-He (engine extension; the reference has none): Hecht & Harting (2010).
 template <class L, int F, class R>
-__device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b) {
+__device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b, R one) {
     constexpr int ax = F / 2;
     constexpr int sgn = (F & 1) ? -1 : 1;   // inward normal sign along ax
-    R s0 = R(0), sout = R(0);
+    R s0 = one, sout = R(0);
     sfor<L::Q>([&](auto I) {
         constexpr int cn = L::c(I, ax) * sgn;
         if constexpr (cn == 0) s0 += f[I];
@@ -503,7 +534,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (leaves<L>(i, F)) {
-                R v = S::ld(P.srcp[i], g.cell, R(L::w(i)));
+                R v = S::ld(P.srcp[i], g.cell);
                 if (kind == BC_BOUNCE_BACK) {
                     R cu = R(0);
 #pragma unroll
@@ -531,13 +562,15 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
                 R cu = R(0);
 #pragma unroll
                 for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
-                f[L::qbar(i)] = -S::ld(P.srcp[i], g.cell, R(L::w(i))) +
-                                R(2) * R(L::w(i)) * rw * (R(1) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
+                // with h = f - w: h[ibar] = -h*[i] + 2 w (rho_w (...) - 1)
+                f[L::qbar(i)] = -S::ld(P.srcp[i], g.cell) +
+                                R(2) * R(L::w(i)) * (rw * (R(1) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3)) -
+                                                     (S::DEV ? R(1) : R(0)));
             }
         });
     } else if (kind == BC_ZOU_HE) {
-        if constexpr (VS == VS_D2Q9) zou_he_d2q9<R>(F, f, b);
-        else if constexpr (VS == VS_D3Q19) zou_he_3d<L, F, R>(f, b);
+        if constexpr (VS == VS_D2Q9) zou_he_d2q9<R>(F, f, b, S::DEV ? R(1) : R(0));
+        else if constexpr (VS == VS_D3Q19) zou_he_3d<L, F, R>(f, b, S::DEV ? R(1) : R(0));
     }
 }
 
@@ -548,7 +581,22 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
     using L = Lat<VS>;
     const SFaceBC& b = P.sface[F];
     const int kind = b.kind;
-    if (kind == SBC_PERIODIC || kind == SBC_ZEROTH || kind == SBC_SECOND) return;
+    if (kind == SBC_PERIODIC) return;
+    if (kind == SBC_ZEROTH || kind == SBC_SECOND) {
+        // extrapolation from the neighbours along the inward normal
+        // (src/passive_scalar/bc.rs:154-199); only the face pass reaches here.
+        const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+        const R* sn = (const R*)P.snap[F];
+        const bool second = kind == SBC_SECOND, all = !b.unknown_only;
+        sfor<L::Q>([&](auto J) {
+            constexpr int j = J;
+            if (all || leaves<L>(L::qbar(j), F)) {
+                const R g1 = sn[(0 * L::Q + j) * pl + pos];
+                gg[j] = second ? R(2) * g1 - sn[(1 * L::Q + j) * pl + pos] : g1;
+            }
+        });
+        return;
+    }
     if (kind == SBC_BB_NO_FLUX) {
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
@@ -594,9 +642,22 @@ __device__ __forceinline__ void apply_faces(const KParams<VS>& P, const Geo& g, 
         const int fr = P.order[O];
         sfor<L::NF>([&](auto FF) {
             constexpr int F = FF;
-            if (fr == F && on_face(g, F, P)) {
-                momentum_face<VS, ST, F>(P, g, f);
-                if constexpr (SCALAR) scalar_face<VS, F, R>(P, g, gg);
+            if (fr == F) {
+                if constexpr (SCALAR) {
+                    // snapshot for an outflow face F, taken where F sits in the face order
+                    if (P.snap[F]) {
+                        const int dist = face_dist(g, F, P);
+                        if (dist == 1 || dist == 2) {
+                            R* sn = (R*)P.snap[F];
+                            const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+                            sfor<L::Q>([&](auto J) { sn[((dist - 1) * L::Q + J) * pl + pos] = gg[J]; });
+                        }
+                    }
+                }
+                if (on_face(g, F, P)) {
+                    momentum_face<VS, ST, F>(P, g, f);
+                    if constexpr (SCALAR) scalar_face<VS, F, R>(P, g, gg);
+                }
             }
         });
     });
@@ -625,45 +686,194 @@ __device__ __forceinline__ bool scalar_source(const StepParams& P, bool bb, R c_
     return true;
 }
 
-// =================================================================== the step
-// MODE: 0 bulk sweep (skips nodes of the face pass), 1 face pass.
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
-__global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
+// Equilibrium, collision and store of the post-collision populations.  BGK and
+// TRT are evaluated one direction (BGK) or one opposite pair (TRT) at a time
+// and stored at once, so only f[] stays live; MRT needs all moments together.
+template <int VS, int COLL, int ST>
+__device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                              typename Store<ST>::R rho, typename Store<ST>::R dr,
+                                              const typename Store<ST>::R* u, typename Store<ST>::R uu,
+                                              const typename Store<ST>::R* F, bool force, long long cell) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
+    constexpr int Q = L::Q;
+    constexpr bool DEV = S::DEV;
+    if constexpr (COLL == COLL_BGK) {
+        const R w1 = R(P.omega), w0 = R(1) - R(P.omega);
+        const R cb = R(1.0 - 0.5 / P.tau);
+        sfor<Q>([&](auto I) {
+            constexpr int i = I;
+            R v = w0 * f[i] + w1 * eq_i<L, DEV, R>(i, rho, dr, u, uu);
+            if (force) v += cb * guo_i<L, R>(i, u, F);
+            S::st(P.dstp[i], cell, v);
+        });
+    } else if constexpr (COLL == COLL_TRT) {
+        const R wp = R(P.op), wm = R(P.om);
+        const bool src = force && P.compat == COMPAT_PHYSICS;
+        const R cp = R(1.0 - 0.5 * P.op), cm = R(1.0 - 0.5 * P.om);
+        sfor<Q>([&](auto I) {
+            constexpr int i = I, ib = L::qbar(i);
+            if constexpr (i <= ib) {
+                const R ei = eq_i<L, DEV, R>(i, rho, dr, u, uu), eb = eq_i<L, DEV, R>(ib, rho, dr, u, uu);
+                const R fp = R(0.5) * (f[i] + f[ib]), fep = R(0.5) * (ei + eb);
+                const R fm = R(0.5) * (f[i] - f[ib]), fem = R(0.5) * (ei - eb);
+                R vi = f[i] - wp * (fp - fep) - wm * (fm - fem);
+                R vb = f[ib] - wp * (fp - fep) - wm * (-fm - -fem);
+                if (src) {
+                    const R si = guo_i<L, R>(i, u, F), sb = guo_i<L, R>(ib, u, F);
+                    vi += cp * R(0.5) * (si + sb) + cm * R(0.5) * (si - sb);
+                    vb += cp * R(0.5) * (sb + si) + cm * R(0.5) * (sb - si);
+                }
+                S::st(P.dstp[i], cell, vi);
+                if constexpr (i != ib) S::st(P.dstp[ib], cell, vb);
+            }
+        });
+    } else {
+        R fe[Q];
+        sfor<Q>([&](auto I) { fe[I] = eq_i<L, DEV, R>(I, rho, dr, u, uu); });
+        collide<VS, COLL, DEV, R>(P, f, fe, rho, dr, u, F, force, P.tau, P.omega, P.op, P.om, P.rates, P.compat);
+        sfor<Q>([&](auto I) { S::st(P.dstp[I], cell, f[I]); });
+    }
+}
+
+// ---- bulk-copy staging (cp.async.bulk into shared memory, mbarrier completion)
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+// One contiguous global -> shared copy; 16-byte aligned addresses, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls (each poll suspends for a
+// hardware-chosen interval) and reports failure instead of hanging.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase, long long limit) {
+    for (long long it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+constexpr long long WAIT_LIMIT = 1ll << 22;
+
+// =================================================================== the step
+// FACEBC: explicit face BCs (else no-slip walls are folded into the link bits).
+// STAGE: one block per x-row; the Q source rows of the pull (and of the scalar)
+// are brought into shared memory by bulk copies issued by one thread, so the
+// bytes in flight do not occupy registers and every global read is a full,
+// aligned line.  Requires blockDim.x == nx and nx * sizeof(T) % 16 == 0.
+// Light kernels (BGK/TRT on D2Q9/D3Q19, FP32 compute, no scalar) are held to 64 registers
+// so that at least 1024 threads fit on an SM; the others may use 128.
+template <int VS, int COLL, int ST, bool SCALAR>
+constexpr int light_kernel() { return COLL != COLL_MRT && VS != VS_D3Q27 && !SCALAR && ST != ST_F64 ? 2 : 1; }
+
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, bool STAGE>
+__global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_kernel<VS, COLL, ST, SCALAR>())
+    k_step(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    using T = typename S::T;
     constexpr int Q = L::Q, D = L::D;
+    constexpr bool DEV = S::DEV;
 
     Geo g;
-    g.x = blockIdx.x * blockDim.x + threadIdx.x;
-    g.y = blockIdx.y;
-    g.z = blockIdx.z;
-    const bool inside = g.x < P.nx;
-    g.cell = (long long)(inside ? g.x : 0) + (long long)P.nx * ((long long)g.y + (long long)P.ny * g.z);
+    bool inside;
+    const bool staged = STAGE && !P.face_pass && !P.first;
+    if (FACEBC && P.face_pass) {
+        // one thread per node of face fp_face
+        const int F = P.fp_face;
+        const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        inside = pos < P.pb_plane[F];
+        const long long pp = inside ? pos : 0;
+        if (F < 2) { g.x = F == 0 ? 0 : P.nx - 1; g.y = (int)(pp % P.ny); g.z = (int)(pp / P.ny); }
+        else if (F < 4) { g.y = F == 2 ? 0 : P.ny - 1; g.x = (int)(pp % P.nx); g.z = (int)(pp / P.nx); }
+        else { g.z = F == 4 ? 0 : P.nz - 1; g.x = (int)(pp % P.nx); g.y = (int)(pp / P.nx); }
+    } else {
+        g.x = blockIdx.x * blockDim.x + threadIdx.x;
+        g.y = blockIdx.y;
+        g.z = blockIdx.z;
+        inside = g.x < P.nx;
+        if (!inside) g.x = 0;
+    }
+    g.cell = (long long)g.x + (long long)P.nx * ((long long)g.y + (long long)P.ny * g.z);
+    g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+    g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+    g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+    g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+    g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+    g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+
+    // ---- stage the source rows of this x-row ------------------------------------
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* rows = (T*)smem_raw;
+    R* grows = (R*)(smem_raw + (size_t)Q * P.nx * sizeof(T));
+    if constexpr (STAGE) {
+        if (staged) {
+            const unsigned rb = (unsigned)(P.nx * sizeof(T));
+            const unsigned grb = SCALAR ? (unsigned)(P.nx * sizeof(R)) : 0u;
+            uint64_t* bar = (uint64_t*)(smem_raw + (size_t)Q * (rb + grb));
+            if (threadIdx.x == 0) mbar_init(bar, 1);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                mbar_expect_tx(bar, Q * (rb + grb));
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I;
+                    // pull source row of direction i: (y - c_iy, z - c_iz), periodic
+                    const int ys = L::c(i, 1) > 0 ? g.ym : (L::c(i, 1) < 0 ? g.yp : g.y);
+                    const int zs = D == 3 ? (L::c(i, 2) > 0 ? g.zm : (L::c(i, 2) < 0 ? g.zp : g.z)) : 0;
+                    const long long row = (long long)P.nx * ((long long)ys + (long long)P.ny * zs);
+                    bulk_g2s(rows + (size_t)i * P.nx, (const T*)P.srcp[i] + row, rb, bar);
+                    if constexpr (SCALAR) bulk_g2s(grows + (size_t)i * P.nx, (const R*)P.gsrcp[i] + row, grb, bar);
+                });
+            }
+            if (!mbar_wait_bounded(bar, 0, WAIT_LIMIT)) {
+                if (threadIdx.x == 0 && P.err) atomicExch(P.err, 1);
+                mbar_wait_bounded(bar, 0, WAIT_LIMIT);   // let the copies in flight land
+                return;
+            }
+        }
+    }
+
     const uint32_t mk = inside ? P.mask[g.cell] : M_SOLID;
-    const bool active = !(mk & M_SOLID);
+    bool active = !(mk & M_SOLID);
+    if constexpr (FACEBC) active = active && ((P.face_pass != 0) == ((mk & M_SKIP) != 0));
 
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (active) {
-        g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
-        g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
-        g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
-        g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
-        g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
-        g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
-
         // ---- stream (pull) + inner bounce-back -------------------------------
         R f[Q];
         if (P.first) {
-            sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], g.cell, R(L::w(I))); });
+            sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], g.cell); });
         } else {
             sfor<Q>([&](auto I) {
                 constexpr int i = I, ib = L::qbar(i);
                 if (mk >> ib & 1u) {
-                    f[i] = S::ld(P.srcp[ib], g.cell, R(L::w(ib)));
+                    f[i] = S::ld(P.srcp[ib], g.cell);   // f[i] = f*[ibar] of this node
+                } else if (STAGE && staged) {
+                    const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
+                    f[i] = S::cvt(rows[(size_t)i * P.nx + xs]);
                 } else {
                     const long long n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
-                    f[i] = S::ld(P.srcp[i], n, R(L::w(i)));
+                    f[i] = S::ld(P.srcp[i], n);
                 }
             });
         }
@@ -684,6 +894,9 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
                             const R cs = P.c_init ? R(P.c_init[n]) : R(P.c_solid);
                             gg[i] = -own + R(2) * R(L::w(ib)) * cs;
                         }
+                    } else if (STAGE && staged) {
+                        const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
+                        gg[i] = grows[(size_t)i * P.nx + xs];
                     } else {
                         gg[i] = ((const R*)P.gsrcp[i])[n];
                     }
@@ -692,12 +905,13 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
         }
         // ---- face boundary conditions ------------------------------------------
         if constexpr (FACEBC) {
-            if (!P.first && (mk & M_FACE)) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+            if (!P.first && (mk & (M_FACE | M_NEAR))) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
         }
 
         // ---- moments (src/momentum/node.rs:418-457) ------------------------------
-        R rho = R(0);
-        sfor<Q>([&](auto I) { rho += f[I]; });
+        R drho = R(0);
+        sfor<Q>([&](auto I) { drho += f[I]; });
+        const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
         R u[3] = {R(0), R(0), R(0)};
         sfor<D>([&](auto A) {
             R s = R(0);
@@ -711,6 +925,7 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
         R F[3] = {R(P.force[0]), R(P.force[1]), R(P.force[2])};
         const bool force = P.has_force != 0;
         if (force) sfor<D>([&](auto A) { u[A] += R(0.5) * F[A] / rho; });
+        const R dr = DEV ? drho : rho - R(1);
 
         // ---- scalar value (src/passive_scalar/node.rs:272-279) --------------------
         R cval = R(0), q = R(0), cst = R(0);
@@ -735,8 +950,8 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
             // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
             if (P.residual) {
                 const R* mp = (const R*)P.mom_prev;
-                const double dr = double(rho) - double(mp[g.cell]);
-                racc[0] = dr * dr;
+                const double d0 = double(rho) - double(mp[g.cell]);
+                racc[0] = d0 * d0;
                 sfor<D>([&](auto A) {
                     const double du = double(u[A]) - double(mp[(1 + A) * P.N + g.cell]);
                     racc[1 + A] = du * du;
@@ -773,10 +988,7 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
             // ---- equilibrium + collision --------------------------------------------
             R uu = R(0);
             sfor<D>([&](auto A) { uu += u[A] * u[A]; });
-            R fe[Q];
-            sfor<Q>([&](auto I) { fe[I] = feq_i<L, R>(I, rho, u, uu); });
-            collide<VS, COLL, R>(P, f, fe, rho, u, F, force, P.tau, P.omega, P.op, P.om, P.rates, P.compat);
-            sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, f[I], R(L::w(I))); });
+            collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, g.cell);
 
             if constexpr (SCALAR) {
                 // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
@@ -808,6 +1020,19 @@ __global__ void __launch_bounds__(256) k_step(const KParams<VS> P) {
                     ((R*)P.cprev)[g.cell] = cval;
                 }
             }
+        }
+    }
+    if (!P.observe && !P.face_pass && !P.first) {
+        // Solid nodes are never read, but storing them when a node in the same
+        // 32-byte sector is fluid turns partial-sector stores (which cost a DRAM
+        // read to fill) into full-sector stores.  Lanes map to consecutive x.
+        constexpr int per = 32 / (int)sizeof(T);
+        const unsigned fl = __ballot_sync(__activemask(), active);
+        const int lane = threadIdx.x & 31;
+        const unsigned grp = (per >= 32 ? 0xffffffffu : ((1u << per) - 1u) << ((lane / per) * per));
+        if (inside && (mk & M_SOLID) && (fl & grp)) {
+            sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
+            if constexpr (SCALAR) sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = R(0); });
         }
     }
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);

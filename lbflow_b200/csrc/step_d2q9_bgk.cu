@@ -1,0 +1,6 @@
+// Step-kernel instantiations for D2Q9 with BGK collision.
+#include "dispatch.cuh"
+
+namespace lbf {
+LBF_INSTANTIATE_COLL(VS_D2Q9, COLL_BGK)
+}  // namespace lbf

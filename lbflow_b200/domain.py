@@ -96,6 +96,15 @@ class Domain:
                                            tol_velocity, tol_scalar, C.byref(steps), _stream_handle(stream)))
         return steps.value
 
+    def set_option(self, option: int, value: int) -> "Domain":
+        _abi.check(self.lib.lbf_domain_set_option(self.h, int(option), int(value)))
+        return self
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        _abi.check(self.lib.lbf_domain_get_option(self.h, int(option), C.byref(v)))
+        return v.value
+
     @property
     def time_step(self) -> int:
         t = C.c_int64()

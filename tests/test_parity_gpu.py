@@ -138,10 +138,10 @@ def test_cavity_d2q9_face_order(Domain):
 
 def test_mrt_d2q9_reference_and_physics(Domain):
     # Reference mode keeps the reference's m_eq of src/velocity_set/d2q9.rs:247-264,
-    # whose energy moments do not match M f_eq: it diverges unless the e and
-    # epsilon rates are 1 (the oracle shows the same), so those rates are 1 here.
+    # whose energy and heat-flux moments do not match M f_eq: it diverges unless
+    # those rates are 1 (the oracle shows the same), so they are 1 here.
     p = cases.cavity_d2q9(20, 0.6, 0.05, Storage.F64)
-    p.collision_operator = MRT([1.0, 1.0, 1.0, 1.0, 1.2, 1.0, 1.2, 1 / 0.6, 1 / 0.6])
+    p.collision_operator = MRT([1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1 / 0.6, 1 / 0.6])
     compare(Domain, p, 500)
     p.collision_operator = MRT([1.0, 1.4, 1.4, 1.0, 1.2, 1.0, 1.2, 1 / 0.6, 1 / 0.6])
     p.compat = Compat.PHYSICS
@@ -274,6 +274,22 @@ def test_scalar_packed_bed_d3q19(Domain):
     compare(Domain, mp, 200, scalar=sp)
 
 
+@pytest.mark.parametrize("kind,unknown", [("zeroth", True), ("zeroth", False), ("second", True),
+                                          ("second", False)])
+def test_scalar_extrapolation_outflow_d2q9(Domain, kind, unknown):
+    mp, sp = _scalar_channel(ps.InnerAntiBounceBack)
+    bc = (ps.ZerothOrderNoFlux if kind == "zeroth" else ps.SecondOrderNoFlux)(unknown_populations_only=unknown)
+    sp.boundary_conditions = [(W, ps.AntiBounceBack(1.0)), (E, bc), (S, ps.BBNoFlux), (N, ps.AntiBBNoFlux)]
+    compare(Domain, mp, 300, scalar=sp)
+
+
+def test_scalar_outflow_with_face_order_d3q19(Domain):
+    mask = cases.sphere_pack([12, 10, 16], 0.8, 1.5, 2.5, seed=8)
+    mp, sp = cases.packed_bed_scalar([12, 10, 16], mask=mask, storage=Storage.F64, ka=1e-2)
+    mp.face_order = [T, B, N, S, E, W]
+    compare(Domain, mp, 150, scalar=sp)
+
+
 # ------------------------------------------------------------------ drivers
 def test_residuals_match_oracle(Domain):
     p = cases.cavity_d2q9(24, 0.6, 0.1, Storage.F64)
@@ -311,6 +327,21 @@ def test_mass_conservation_and_solve_path(Domain):
     assert abs(inv1[0] - inv0[0]) <= 1e-10 * inv0[0]
     r2, u2, _ = solve_arrays(p, 400)
     assert np.array_equal(r1, r2) and np.array_equal(u1, u2)
+
+
+@pytest.mark.parametrize("storage", [Storage.F64, Storage.F32, Storage.F16DEV])
+def test_staged_and_unstaged_sweeps_agree(Domain, storage):
+    """The bulk-copy staged sweep and the plain-load sweep compute identical results."""
+    mask = cases.sphere_pack([32, 20, 16], 0.75, 2.0, 3.5, seed=13)
+    p = cases.porous_channel_d3q19([32, 20, 16], mask=mask, force=1e-5, storage=storage)
+    out = []
+    for stage in (1, 0):
+        with Domain(p) as gd:
+            gd.set_option(_abi.LBF_OPT_STAGE, stage)
+            assert gd.get_option(_abi.LBF_OPT_STAGE) == stage
+            gd.init().step(60)
+            out.append(gd.moments())
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
 
 
 @pytest.mark.parametrize("storage,tol", [(Storage.F16DEV, 3e-2), (Storage.BF16DEV, 2e-1)])
