@@ -222,6 +222,25 @@ lbf_status lbf_domain_time_step(lbf_domain* dom, int64_t* t);
 lbf_status lbf_domain_device_bytes(lbf_domain* dom, int64_t* bytes);
 lbf_status lbf_domain_destroy(lbf_domain* dom);
 
+/* ---- FP64 fluid sums with no device allocation --------------------------- */
+/* No counterpart in the reference (whose reductions are rayon sums on the CPU).
+ * For callers that cannot allocate device memory when they need the sums: code
+ * inside a CUDA stream capture, where allocation calls are not allowed, or hosts
+ * whose HBM is already reserved by their own allocator or by lattices sized to
+ * fill it.  Computes [sum rho, sum rho*u_a (d values), sum C, sum q_ads] over the
+ * nodes whose node_class lacks LBF_CLASS_SOLID, from caller-owned device arrays
+ * (density[n], velocity[n*d], optional scalar[n] and q_ads[n], node_class[n] as
+ * returned by lbf_domain_get_node_class), into the caller-owned device array
+ * out[3 + d].  Scratch lives in a fixed 16 KiB static device array that every
+ * GPU loading the library holds until exit; each call clears it first, and calls
+ * that overlap on the GPU race on it.  The first call on a device looks up that
+ * array's address (cudaGetSymbolAddress) with the device current: make it before
+ * any stream capture.  Rejects n > LBF_NOALLOC_MAX_NODES and d outside {2, 3}. */
+#define LBF_NOALLOC_MAX_NODES 2147483647LL
+lbf_status lbf_inventory_noalloc(const double* density, const double* velocity, const double* scalar,
+                                 const double* q_ads, const uint32_t* node_class, int64_t n, int32_t d,
+                                 double* out, void* stream);
+
 /* ---- whole solve with host buffers (the `lbflow::solve` drop-in) --------- */
 /* Creates a domain from `desc` (+ optional scalar), initialises it, runs
  * `nsteps` main_steps and copies the final moments to the host arrays.

@@ -105,6 +105,7 @@ SIGNATURES = {
     "lbf_domain_device_bytes": (_I32, [_P, _PI64]),
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),
+    "lbf_inventory_noalloc": (_I32, [_P, _P, _P, _P, _P, _I64, _I32, _P, _P]),
 }
 
 _LIB_NAME = "liblbflow_b200.so"

@@ -524,6 +524,11 @@ lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
 
 }  // namespace
 
+// Lets the other translation units of the library report through lbf_last_error().
+__attribute__((visibility("hidden"))) lbf_status lbf_internal_fail(lbf_status s, const char* msg) {
+    return fail(s, msg);
+}
+
 // ============================================================== C API
 extern "C" {
 
