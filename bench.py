@@ -48,7 +48,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block", type=int, default=0, help="override the x block size")
-    ap.add_argument("--no-stage", action="store_true", help="plain-load sweep instead of bulk-copy staging")
+    ap.add_argument("--sweep", default="plain", choices=["pipe", "stage", "plain"],
+                    help="pipelined bulk-copy sweep, one-shot staged sweep, or plain loads")
+    ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
     return ap.parse_args()
 
 
@@ -206,9 +208,12 @@ def run_engine(args, rank, world, local_rank):
     dom = Domain(p)
     if args.block:
         dom.set_option(_abi.LBF_OPT_BLOCK_X, args.block)
-    if args.no_stage:
-        dom.set_option(_abi.LBF_OPT_STAGE, 0)
-    staged = bool(dom.get_option(_abi.LBF_OPT_STAGE))
+    dom.set_option(_abi.LBF_OPT_PIPE, 1 if args.sweep == "pipe" else 0)
+    dom.set_option(_abi.LBF_OPT_STAGE, 1 if args.sweep == "stage" else 0)
+    if args.stages:
+        dom.set_option(_abi.LBF_OPT_PIPE_STAGES, args.stages)
+    sweep = ("pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
+             "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else "plain loads")
     dom.init(stream)
     dom.step(args.warmup, 0, stream)
     torch.cuda.synchronize()
@@ -270,7 +275,7 @@ def run_engine(args, rank, world, local_rank):
             "config": {"workload": workload_name(args), "storage": args.storage, "n_fluid": n_fluid,
                        "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
                        "parallelism": "replicas" if world > 1 else "single",
-                       "sweep": "bulk-copy staged" if staged else "plain loads"},
+                       "sweep": sweep},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},

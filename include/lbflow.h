@@ -210,10 +210,13 @@ lbf_status lbf_domain_inventory(lbf_domain* dom, double* out, void* stream);
 lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint32_t* links);
 /* Launch options (no reference counterpart; used by the autotuner):
  * LBF_OPT_BLOCK_X  threads per block along x for the unstaged sweep (0 = heuristic)
- * LBF_OPT_STAGE    1 = stage the pull rows in shared memory with bulk copies when the
- *                  shape allows it (nx <= 512, rows 16-byte aligned); 0 = plain loads.
- * lbf_domain_get_option(LBF_OPT_STAGE) reports whether staging is in effect. */
-enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1 };
+ * LBF_OPT_STAGE    1 = one-shot staging of the pull rows in shared memory with bulk
+ *                  copies when the shape allows it (nx <= 512, rows 16-byte aligned).
+ * LBF_OPT_PIPE     1 = pipelined bulk-copy sweep on the lean path (faces periodic or
+ *                  no-slip, no scalar, rows 16-byte aligned); default 0 (plain loads).
+ * LBF_OPT_PIPE_STAGES  ring depth of the pipelined sweep (0 = from the smem budget).
+ * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
+enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */

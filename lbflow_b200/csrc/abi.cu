@@ -156,7 +156,9 @@ struct lbf_domain {
     long long t = 0;
     long long res_step = -1;
     int block_x = 0;
-    bool stage = true;            // use the bulk-copy staged sweep when the shape allows it
+    bool stage = false;           // one-shot staged sweep (off: the pipelined sweep supersedes it)
+    bool pipe = false;            // pipelined bulk-copy sweep on the lean path (option)
+    int pipe_stages = 0;          // 0 = chosen from the shared-memory budget
     int* err = nullptr;           // device flag: a bounded wait gave up
     cudaStream_t last_stream = nullptr;
     long long bytes = 0;
@@ -408,8 +410,42 @@ bool can_stage(const lbf_domain* D) {
     return stage_smem(D->q, D->n[0], tb, rb, D->scalar) <= 200 * 1024;
 }
 
+// Whether the pipelined sweep applies (lean path, aligned rows, two stages fit).
+bool can_pipe(const lbf_domain* D) {
+    const size_t rowb = D->n[0] * st_bytes(D->st);
+    return !D->facebc && !D->scalar && rowb % 16 == 0 && 2 * D->q * rowb <= 200 * 1024;
+}
+
+cudaError_t launch_pipe(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    const size_t stage_b = (size_t)D->q * D->n[0] * st_bytes(D->st);
+    // three blocks of <= 288 threads per SM share ~220 KB of shared memory
+    int stages = D->pipe_stages > 0 ? D->pipe_stages : (int)std::max<size_t>(2, std::min<size_t>(8, (72 * 1024) / stage_b));
+    while (stages > 2 && stages * stage_b > 200 * 1024) --stages;
+    const int nc = (int)std::min<long long>(8, std::max<long long>(1, (D->n[0] + 31) / 32));
+    const int coll = D->desc.collision.kind;
+    switch (D->vs) {
+        case LBF_D2Q9:
+            return coll == LBF_BGK ? launch_step_pipe<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, stages, nc, s)
+                 : coll == LBF_TRT ? launch_step_pipe<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, stages, nc, s)
+                                   : launch_step_pipe<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, stages, nc, s);
+        case LBF_D3Q19:
+            return coll == LBF_BGK ? launch_step_pipe<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, stages, nc, s)
+                 : coll == LBF_TRT ? launch_step_pipe<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, stages, nc, s)
+                                   : launch_step_pipe<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, stages, nc, s);
+        default:
+            return coll == LBF_BGK ? launch_step_pipe<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), stages, nc, s)
+                 : coll == LBF_TRT ? launch_step_pipe<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), stages, nc, s)
+                                   : launch_step_pipe<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), stages, nc, s);
+    }
+}
+
 // The bulk sweep, then one face pass per scalar outflow face.
 cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    if (D->pipe && can_pipe(D) && !P.first && !P.observe && !P.face_pass) {
+        cudaError_t e = launch_pipe(D, P, s);
+        if (e != cudaErrorNotSupported) return e;
+        cudaGetLastError();
+    }
     const bool stage = D->stage && can_stage(D);
     const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
     cudaError_t e = launch_one(D, P, stage, Launch{step_grid(D, b), b, s});
@@ -811,6 +847,13 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
         case LBF_OPT_STAGE:
             D->stage = value != 0;
             return LBF_OK;
+        case LBF_OPT_PIPE:
+            D->pipe = value != 0;
+            return LBF_OK;
+        case LBF_OPT_PIPE_STAGES:
+            if (value < 0 || value == 1 || value > 16) return fail(LBF_EINVAL, "pipeline stages must be 0 (auto) or 2..16");
+            D->pipe_stages = (int)value;
+            return LBF_OK;
         default:
             return fail(LBF_EINVAL, "unknown option");
     }
@@ -821,6 +864,8 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
     switch (option) {
         case LBF_OPT_BLOCK_X: *value = D->block_x; return LBF_OK;
         case LBF_OPT_STAGE: *value = (D->stage && can_stage(D)) ? 1 : 0; return LBF_OK;
+        case LBF_OPT_PIPE: *value = (D->pipe && can_pipe(D)) ? 1 : 0; return LBF_OK;
+        case LBF_OPT_PIPE_STAGES: *value = D->pipe_stages; return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
     }
 }

@@ -2,6 +2,8 @@
 // (step_d2q9.cu, step_d3q19.cu, step_d3q27.cu instantiate them).
 #pragma once
 
+#include <algorithm>
+
 #include "aux_kernels.cuh"
 
 namespace lbf {
@@ -58,6 +60,36 @@ inline void fill_lam(KParams<VS_D3Q27>& kp, const double* lam) {
     LBF_STEP_ST(C_, ST_F64) LBF_STEP_ST(C_, ST_F32) LBF_STEP_ST(C_, ST_F16) LBF_STEP_ST(C_, ST_BF16) \
     LBF_STEP_CASE(C_, ST_F64, true, true) LBF_STEP_CASE(C_, ST_F32, true, true)
 
+// Pipelined sweep (lean path only); returns cudaErrorNotSupported when the shape
+// does not allow it (the caller then uses k_step).
+template <int VS, int COLL>
+cudaError_t launch_step_pipe(int st, const StepParams& base, const double* lam, int stages, int nc,
+                             cudaStream_t stream);
+
+template <int VS, int COLL, int ST>
+cudaError_t launch_pipe_st(const KParams<VS>& kp, int stages, int nc, cudaStream_t stream) {
+    using T = typename Store<ST>::T;
+    const size_t smem = (size_t)stages * Lat<VS>::Q * kp.nx * sizeof(T) + 2 * stages * sizeof(uint64_t);
+    const int threads = 32 * (1 + nc);
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_step_pipe<VS, COLL, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        smem_set = smem;
+    }
+    int per_sm = 0, dev = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_pipe<VS, COLL, ST>, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorNotSupported;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long rows = (long long)kp.ny * kp.nz;
+    const long long blocks = std::min<long long>(rows, (long long)per_sm * sms);
+    k_step_pipe<VS, COLL, ST><<<(unsigned)blocks, threads, smem, stream>>>(kp);
+    return cudaGetLastError();
+}
+
 // One translation unit per (velocity set, collision) instantiates the step kernels.
 template <int VS, int COLL>
 cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const StepParams& base, const double* lam,
@@ -74,6 +106,22 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
         fill_lam(kp, lam);                                                                             \
         LBF_STEP_COLL(COLL_)                                                                           \
         return cudaErrorInvalidValue;                                                                  \
+    }                                                                                                  \
+    template <>                                                                                        \
+    cudaError_t launch_step_pipe<VS_, COLL_>(int st, const StepParams& base, const double* lam,         \
+                                             int stages, int nc, cudaStream_t stream) {                 \
+        KParams<VS_> kp;                                                                               \
+        static_cast<StepParams&>(kp) = base;                                                           \
+        fill_lam(kp, lam);                                                                             \
+        kp.pipe_stages = stages;                                                                       \
+        kp.pipe_nc = nc;                                                                               \
+        switch (st) {                                                                                  \
+            case ST_F64: return launch_pipe_st<VS_, COLL_, ST_F64>(kp, stages, nc, stream);            \
+            case ST_F32: return launch_pipe_st<VS_, COLL_, ST_F32>(kp, stages, nc, stream);            \
+            case ST_F16: return launch_pipe_st<VS_, COLL_, ST_F16>(kp, stages, nc, stream);            \
+            case ST_BF16: return launch_pipe_st<VS_, COLL_, ST_BF16>(kp, stages, nc, stream);          \
+            default: return cudaErrorInvalidValue;                                                     \
+        }                                                                                              \
     }
 
 #define LBF_INSTANTIATE(VS_)                                                                           \

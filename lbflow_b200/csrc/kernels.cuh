@@ -86,6 +86,7 @@ struct StepParams {
     int observe, write_mom, residual;
     int face_pass, fp_face;   // face pass: update the nodes of face fp_face only
     int* err;                 // set to 1 when a bounded wait gives up
+    int pipe_stages, pipe_nc; // pipelined sweep: ring stages, consumer warps
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -137,48 +138,57 @@ struct Store<ST_F64> {
     using T = double;
     using R = double;
     static constexpr bool DEV = false;
-    __device__ static __forceinline__ R ld(const void* p, long long o) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
-    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = v; }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
 };
 template <>
 struct Store<ST_F32> {
     using T = float;
     using R = float;
     static constexpr bool DEV = true;
-    __device__ static __forceinline__ R ld(const void* p, long long o) { return ((const T*)p)[o]; }
+    __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
-    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = v; }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
 };
 template <>
 struct Store<ST_F16> {
     using T = __half;
     using R = float;
     static constexpr bool DEV = true;
-    __device__ static __forceinline__ R ld(const void* p, long long o) { return __half2float(((const T*)p)[o]); }
+    __device__ static __forceinline__ R ld(const void* p, int o) { return __half2float(((const T*)p)[o]); }
     __device__ static __forceinline__ R cvt(T v) { return __half2float(v); }
-    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = __float2half_rn(v); }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v); }
 };
 template <>
 struct Store<ST_BF16> {
     using T = __nv_bfloat16;
     using R = float;
     static constexpr bool DEV = true;
-    __device__ static __forceinline__ R ld(const void* p, long long o) { return __bfloat162float(((const T*)p)[o]); }
+    __device__ static __forceinline__ R ld(const void* p, int o) { return __bfloat162float(((const T*)p)[o]); }
     __device__ static __forceinline__ R cvt(T v) { return __bfloat162float(v); }
-    __device__ static __forceinline__ void st(void* p, long long o, R v) { ((T*)p)[o] = __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2bfloat16_rn(v); }
 };
 
 // ---- node geometry -----------------------------------------------------------
+// Node coordinates, their periodic neighbours, and the 32-bit index offsets of
+// the -1/+1 neighbours along each axis (N < 2^31, so one IADD3 per direction).
 struct Geo {
     int x, y, z;
     int xm, xp, ym, yp, zm, zp;
-    long long cell;
-    __device__ __forceinline__ long long at(int dx, int dy, int dz, const StepParams& P) const {
-        const int xx = dx < 0 ? xm : (dx > 0 ? xp : x);
-        const int yy = dy < 0 ? ym : (dy > 0 ? yp : y);
-        const int zz = dz < 0 ? zm : (dz > 0 ? zp : z);
-        return (long long)xx + (long long)P.nx * ((long long)yy + (long long)P.ny * zz);
+    int cell;
+    int oxm, oxp, oym, oyp, ozm, ozp;
+    __device__ __forceinline__ void offsets(const StepParams& P) {
+        oxm = xm - x;
+        oxp = xp - x;
+        oym = (ym - y) * P.nx;
+        oyp = (yp - y) * P.nx;
+        ozm = (zm - z) * P.nx * P.ny;
+        ozp = (zp - z) * P.nx * P.ny;
+    }
+    __device__ __forceinline__ int at(int dx, int dy, int dz, const StepParams&) const {
+        return cell + (dx < 0 ? oxm : (dx > 0 ? oxp : 0)) + (dy < 0 ? oym : (dy > 0 ? oyp : 0)) +
+               (dz < 0 ? ozm : (dz > 0 ? ozp : 0));
     }
 };
 
@@ -712,12 +722,24 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
         const R wp = R(P.op), wm = R(P.om);
         const bool src = force && P.compat == COMPAT_PHYSICS;
         const R cp = R(1.0 - 0.5 * P.op), cm = R(1.0 - 0.5 * P.om);
+        // for an opposite pair (i, ibar), c_ibar.u = -c_i.u: the symmetric part of the
+        // equilibrium is w (base + rho (4.5 (c.u)^2 - 1.5 u.u)), the antisymmetric 3 w rho c.u
+        const R base = DEV ? dr : rho;
+        const R ruu = R(1.5) * rho * uu;
         sfor<Q>([&](auto I) {
             constexpr int i = I, ib = L::qbar(i);
             if constexpr (i <= ib) {
-                const R ei = eq_i<L, DEV, R>(i, rho, dr, u, uu), eb = eq_i<L, DEV, R>(ib, rho, dr, u, uu);
-                const R fp = R(0.5) * (f[i] + f[ib]), fep = R(0.5) * (ei + eb);
-                const R fm = R(0.5) * (f[i] - f[ib]), fem = R(0.5) * (ei - eb);
+                R cu = R(0);
+                sfor<L::D>([&](auto A) {
+                    constexpr int c = L::c(i, A);
+                    if constexpr (c == 1) cu += u[A];
+                    else if constexpr (c == -1) cu -= u[A];
+                });
+                const R wi = R(L::w(i));
+                const R fep = wi * (base + R(4.5) * rho * cu * cu - ruu);
+                const R fem = wi * R(3) * rho * cu;
+                const R fp = R(0.5) * (f[i] + f[ib]);
+                const R fm = R(0.5) * (f[i] - f[ib]);
                 R vi = f[i] - wp * (fp - fep) - wm * (fm - fem);
                 R vb = f[ib] - wp * (fp - fep) - wm * (-fm - -fem);
                 if (src) {
@@ -756,6 +778,9 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned phase) {
     unsigned ok;
     asm volatile(
@@ -773,6 +798,139 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
     return false;
 }
 constexpr long long WAIT_LIMIT = 1ll << 22;
+
+// Everything a fluid node does after its populations were pulled: face BCs,
+// moments, residual/observe/face-layer outputs, collision + store, and the
+// scalar step.  Shared by the single-pass sweep and the pipelined sweep.
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                             typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                             typename Store<ST>::R* gg, double (&racc)[5]) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    constexpr bool DEV = S::DEV;
+    // ---- face boundary conditions ------------------------------------------
+    if constexpr (FACEBC) {
+        if (!P.first && (mk & (M_FACE | M_NEAR))) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+    }
+
+    // ---- moments (src/momentum/node.rs:418-457) ------------------------------
+    R drho = R(0);
+    sfor<Q>([&](auto I) { drho += f[I]; });
+    const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
+    const R inv_rho = R(1) / rho;
+    R u[3] = {R(0), R(0), R(0)};
+    sfor<D>([&](auto A) {
+        R s = R(0);
+        sfor<Q>([&](auto I) {
+            constexpr int c = L::c(I, A);
+            if constexpr (c == 1) s += f[I];
+            else if constexpr (c == -1) s -= f[I];
+        });
+        u[A] = s * inv_rho;
+    });
+    R F[3] = {R(P.force[0]), R(P.force[1]), R(P.force[2])};
+    const bool force = P.has_force != 0;
+    if (force) sfor<D>([&](auto A) { u[A] += R(0.5) * F[A] * inv_rho; });
+    const R dr = DEV ? drho : rho - R(1);
+
+    // ---- scalar value (src/passive_scalar/node.rs:272-279) --------------------
+    R cval = R(0), q = R(0), cst = R(0);
+    const bool bb = (mk & M_BB) != 0;
+    if constexpr (SCALAR) {
+        R s = R(0);
+        sfor<Q>([&](auto I) { s += gg[I]; });
+        if (P.s_ads && bb) {
+            q = ((const R*)P.qads)[g.cell];
+            cst = ((const R*)P.cprev)[g.cell];
+        }
+        R src;
+        if (scalar_source<R>(P, bb, cst, q, !P.observe, src)) s += R(0.5) * src;
+        cval = s;
+    }
+
+    if (P.observe) {
+        P.obs_rho[g.cell] = double(rho);
+        sfor<D>([&](auto A) { P.obs_u[(long long)g.cell * D + A] = double(u[A]); });
+        if constexpr (SCALAR) P.obs_c[g.cell] = double(cval);
+    } else {
+        // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
+        if (P.residual) {
+            const R* mp = (const R*)P.mom_prev;
+            const double d0 = double(rho) - double(mp[g.cell]);
+            racc[0] += d0 * d0;
+            sfor<D>([&](auto A) {
+                const double du = double(u[A]) - double(mp[(1 + A) * P.N + g.cell]);
+                racc[1 + A] += du * du;
+            });
+            if constexpr (SCALAR) {
+                const double dc = double(cval) - double(mp[(1 + D) * P.N + g.cell]);
+                racc[4] += dc * dc;
+            }
+        }
+        if (P.write_mom) {
+            R* mc = (R*)P.mom_cur;
+            mc[g.cell] = rho;
+            sfor<D>([&](auto A) { mc[(1 + A) * P.N + g.cell] = u[A]; });
+            if constexpr (SCALAR) mc[(1 + D) * P.N + g.cell] = cval;
+        }
+        // ---- previous-step layers next to faces (anti-BB, extrapolation) ---------
+        if constexpr (FACEBC) {
+            if (P.any_face) {
+                sfor<L::NF>([&](auto FF) {
+                    constexpr int Fc = FF;
+                    if (P.pb_dst[Fc]) {
+                        const int dist = face_dist(g, Fc, P);
+                        if (dist <= 1) {
+                            R* pb = (R*)P.pb_dst[Fc];
+                            const long long pl = P.pb_plane[Fc], pos = face_pos(g, Fc, P);
+                            sfor<D>([&](auto A) { pb[(dist * (D + 1) + A) * pl + pos] = u[A]; });
+                            pb[(dist * (D + 1) + D) * pl + pos] = cval;
+                        }
+                    }
+                });
+            }
+        }
+
+        // ---- equilibrium + collision --------------------------------------------
+        R uu = R(0);
+        sfor<D>([&](auto A) { uu += u[A] * u[A]; });
+        collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, g.cell);
+
+        if constexpr (SCALAR) {
+            // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
+            R ge[Q];
+            sfor<Q>([&](auto I) { ge[I] = feq_i<L, R>(I, cval, u, uu); });
+            if (P.s_coll == COLL_BGK) {
+                const R w1 = R(P.s_omega), w0 = R(1) - R(P.s_omega);
+                R src;
+                const bool has = scalar_source<R>(P, bb, cval, q, true, src);
+                const R cb = R(1.0 - 0.5 / P.s_tau);
+                sfor<Q>([&](auto I) {
+                    R v = w0 * gg[I] + w1 * ge[I];
+                    if (has) v += cb * R(L::w(I)) * src;
+                    gg[I] = v;
+                });
+            } else {   // TRT, no source (src/lib.rs:118-127)
+                const R wp = R(P.s_op), wm = R(P.s_om);
+                R out[Q];
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    out[i] = gg[i] - wp * (R(0.5) * (gg[i] + gg[ib]) - R(0.5) * (ge[i] + ge[ib])) -
+                             wm * (R(0.5) * (gg[i] - gg[ib]) - R(0.5) * (ge[i] - ge[ib]));
+                });
+                sfor<Q>([&](auto I) { gg[I] = out[I]; });
+            }
+            sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = gg[I]; });
+            if (P.s_ads && bb) {
+                ((R*)P.qads)[g.cell] = q;
+                ((R*)P.cprev)[g.cell] = cval;
+            }
+        }
+    }
+}
 
 // =================================================================== the step
 // FACEBC: explicit face BCs (else no-slip walls are folded into the link bits).
@@ -793,7 +951,6 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
     using R = typename S::R;
     using T = typename S::T;
     constexpr int Q = L::Q, D = L::D;
-    constexpr bool DEV = S::DEV;
 
     Geo g;
     bool inside;
@@ -814,13 +971,14 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         inside = g.x < P.nx;
         if (!inside) g.x = 0;
     }
-    g.cell = (long long)g.x + (long long)P.nx * ((long long)g.y + (long long)P.ny * g.z);
+    g.cell = g.x + P.nx * (g.y + P.ny * g.z);
     g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
     g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
     g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
     g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
     g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
     g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+    g.offsets(P);
 
     // ---- stage the source rows of this x-row ------------------------------------
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -864,18 +1022,33 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         if (P.first) {
             sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], g.cell); });
         } else {
-            sfor<Q>([&](auto I) {
-                constexpr int i = I, ib = L::qbar(i);
-                if (mk >> ib & 1u) {
-                    f[i] = S::ld(P.srcp[ib], g.cell);   // f[i] = f*[ibar] of this node
-                } else if (STAGE && staged) {
+            auto nb = [&](auto I) {
+                constexpr int i = I;
+                return g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
+            };
+            // a warp whose nodes have no solid or wall links pulls without any test
+            const bool nolinks = __all_sync(__activemask(), !(mk & M_LINKS));
+            if (STAGE && staged) {
+                auto pull = [&](auto I) {
+                    constexpr int i = I;
                     const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
-                    f[i] = S::cvt(rows[(size_t)i * P.nx + xs]);
-                } else {
-                    const long long n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
-                    f[i] = S::ld(P.srcp[i], n);
-                }
-            });
+                    return S::cvt(rows[i * P.nx + xs]);
+                };
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    f[i] = (mk >> ib & 1u) ? S::ld(P.srcp[ib], g.cell) : pull(I);
+                });
+            } else if (nolinks) {
+                sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], nb(I)); });
+            } else {
+                // branch-free: a linked direction reads f*[ibar] of this node (inner
+                // bounce-back / folded wall), the others the pull source
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    const bool lk = (mk >> ib) & 1u;
+                    f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? g.cell : nb(I));
+                });
+            }
         }
         // scalar populations: pull + inner BC (src/passive_scalar/lattice.rs:274-297)
         R gg[SCALAR ? Q : 1];
@@ -885,7 +1058,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
             } else {
                 sfor<Q>([&](auto I) {
                     constexpr int i = I, ib = L::qbar(i);
-                    const long long n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
+                    const int n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
                     if (mk >> ib & 1u) {
                         const R own = ((const R*)P.gsrcp[ib])[g.cell];
                         if (P.s_inner == 1) {
@@ -903,124 +1076,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
                 });
             }
         }
-        // ---- face boundary conditions ------------------------------------------
-        if constexpr (FACEBC) {
-            if (!P.first && (mk & (M_FACE | M_NEAR))) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
-        }
-
-        // ---- moments (src/momentum/node.rs:418-457) ------------------------------
-        R drho = R(0);
-        sfor<Q>([&](auto I) { drho += f[I]; });
-        const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
-        R u[3] = {R(0), R(0), R(0)};
-        sfor<D>([&](auto A) {
-            R s = R(0);
-            sfor<Q>([&](auto I) {
-                constexpr int c = L::c(I, A);
-                if constexpr (c == 1) s += f[I];
-                else if constexpr (c == -1) s -= f[I];
-            });
-            u[A] = s / rho;
-        });
-        R F[3] = {R(P.force[0]), R(P.force[1]), R(P.force[2])};
-        const bool force = P.has_force != 0;
-        if (force) sfor<D>([&](auto A) { u[A] += R(0.5) * F[A] / rho; });
-        const R dr = DEV ? drho : rho - R(1);
-
-        // ---- scalar value (src/passive_scalar/node.rs:272-279) --------------------
-        R cval = R(0), q = R(0), cst = R(0);
-        const bool bb = (mk & M_BB) != 0;
-        if constexpr (SCALAR) {
-            R s = R(0);
-            sfor<Q>([&](auto I) { s += gg[I]; });
-            if (P.s_ads && bb) {
-                q = ((const R*)P.qads)[g.cell];
-                cst = ((const R*)P.cprev)[g.cell];
-            }
-            R src;
-            if (scalar_source<R>(P, bb, cst, q, !P.observe, src)) s += R(0.5) * src;
-            cval = s;
-        }
-
-        if (P.observe) {
-            P.obs_rho[g.cell] = double(rho);
-            sfor<D>([&](auto A) { P.obs_u[g.cell * D + A] = double(u[A]); });
-            if constexpr (SCALAR) P.obs_c[g.cell] = double(cval);
-        } else {
-            // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
-            if (P.residual) {
-                const R* mp = (const R*)P.mom_prev;
-                const double d0 = double(rho) - double(mp[g.cell]);
-                racc[0] = d0 * d0;
-                sfor<D>([&](auto A) {
-                    const double du = double(u[A]) - double(mp[(1 + A) * P.N + g.cell]);
-                    racc[1 + A] = du * du;
-                });
-                if constexpr (SCALAR) {
-                    const double dc = double(cval) - double(mp[(1 + D) * P.N + g.cell]);
-                    racc[4] = dc * dc;
-                }
-            }
-            if (P.write_mom) {
-                R* mc = (R*)P.mom_cur;
-                mc[g.cell] = rho;
-                sfor<D>([&](auto A) { mc[(1 + A) * P.N + g.cell] = u[A]; });
-                if constexpr (SCALAR) mc[(1 + D) * P.N + g.cell] = cval;
-            }
-            // ---- previous-step layers next to faces (anti-BB, extrapolation) ---------
-            if constexpr (FACEBC) {
-                if (P.any_face) {
-                    sfor<L::NF>([&](auto FF) {
-                        constexpr int Fc = FF;
-                        if (P.pb_dst[Fc]) {
-                            const int dist = face_dist(g, Fc, P);
-                            if (dist <= 1) {
-                                R* pb = (R*)P.pb_dst[Fc];
-                                const long long pl = P.pb_plane[Fc], pos = face_pos(g, Fc, P);
-                                sfor<D>([&](auto A) { pb[(dist * (D + 1) + A) * pl + pos] = u[A]; });
-                                pb[(dist * (D + 1) + D) * pl + pos] = cval;
-                            }
-                        }
-                    });
-                }
-            }
-
-            // ---- equilibrium + collision --------------------------------------------
-            R uu = R(0);
-            sfor<D>([&](auto A) { uu += u[A] * u[A]; });
-            collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, g.cell);
-
-            if constexpr (SCALAR) {
-                // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
-                R ge[Q];
-                sfor<Q>([&](auto I) { ge[I] = feq_i<L, R>(I, cval, u, uu); });
-                if (P.s_coll == COLL_BGK) {
-                    const R w1 = R(P.s_omega), w0 = R(1) - R(P.s_omega);
-                    R src;
-                    const bool has = scalar_source<R>(P, bb, cval, q, true, src);
-                    const R cb = R(1.0 - 0.5 / P.s_tau);
-                    sfor<Q>([&](auto I) {
-                        R v = w0 * gg[I] + w1 * ge[I];
-                        if (has) v += cb * R(L::w(I)) * src;
-                        gg[I] = v;
-                    });
-                } else {   // TRT, no source (src/lib.rs:118-127)
-                    const R wp = R(P.s_op), wm = R(P.s_om);
-                    R out[Q];
-                    sfor<Q>([&](auto I) {
-                        constexpr int i = I, ib = L::qbar(i);
-                        out[i] = gg[i] - wp * (R(0.5) * (gg[i] + gg[ib]) - R(0.5) * (ge[i] + ge[ib])) -
-                                 wm * (R(0.5) * (gg[i] - gg[ib]) - R(0.5) * (ge[i] - ge[ib]));
-                    });
-                    sfor<Q>([&](auto I) { gg[I] = out[I]; });
-                }
-                sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = gg[I]; });
-                if (P.s_ads && bb) {
-                    ((R*)P.qads)[g.cell] = q;
-                    ((R*)P.cprev)[g.cell] = cval;
-                }
-            }
-        }
+        process_cell<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc);
     }
     if (!P.observe && !P.face_pass && !P.first) {
         // Solid nodes are never read, but storing them when a node in the same
@@ -1036,6 +1092,128 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         }
     }
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+}
+
+// =================================================================== pipelined sweep
+// Persistent blocks for the lean path (periodic / no-slip faces, no scalar).
+// Warp 0 is the producer: one lane streams the Q source rows of each x-row the
+// block owns (rows r = blockIdx.x + k * gridDim.x) into a ring of pipe_stages
+// shared-memory stages with cp.async.bulk, each stage completing on its `full`
+// mbarrier.  Warps 1..pipe_nc consume: wait on `full`, pull from the stage,
+// collide, store, and release the stage on its `empty` mbarrier.  Several rows
+// of copies are in flight per block at all times without occupying registers.
+// Every wait is bounded; a timeout sets P.err and the block stops early.
+template <int VS, int COLL, int ST>
+__global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    using T = typename S::T;
+    constexpr int Q = L::Q, D = L::D;
+    const int NS = P.pipe_stages, NC = P.pipe_nc;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const unsigned rb = (unsigned)(P.nx * sizeof(T));
+    const size_t stage_bytes = (size_t)Q * rb;
+    uint64_t* full = (uint64_t*)(smem_raw + NS * stage_bytes);
+    uint64_t* empty = full + NS;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NC);
+        }
+    }
+    __syncthreads();
+    const long long nrows = (long long)P.ny * P.nz;
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+
+    if (warp == 0) {
+        if (lane == 0) {
+            long long k = 0;
+            bool failed = false;
+            for (long long r = blockIdx.x; r < nrows; r += gridDim.x, ++k) {
+                const int s = (int)(k % NS);
+                const long long use = k / NS;
+                if (use > 0 && !mbar_wait_bounded(&empty[s], (unsigned)((use - 1) & 1), WAIT_LIMIT)) {
+                    failed = true;
+                    break;
+                }
+                mbar_expect_tx(&full[s], Q * rb);
+                const int y = (int)(r % P.ny), z = (int)(r / P.ny);
+                const int ym = y == 0 ? P.ny - 1 : y - 1, yp = y == P.ny - 1 ? 0 : y + 1;
+                const int zm = z == 0 ? P.nz - 1 : z - 1, zp = z == P.nz - 1 ? 0 : z + 1;
+                T* st = (T*)(smem_raw + s * stage_bytes);
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I;
+                    const int ys = L::c(i, 1) > 0 ? ym : (L::c(i, 1) < 0 ? yp : y);
+                    const int zs = D == 3 ? (L::c(i, 2) > 0 ? zm : (L::c(i, 2) < 0 ? zp : z)) : 0;
+                    const long long row = (long long)P.nx * ((long long)ys + (long long)P.ny * zs);
+                    bulk_g2s(st + (size_t)i * P.nx, (const T*)P.srcp[i] + row, rb, &full[s]);
+                });
+            }
+            // the copies of the last stages must land before the block may exit
+            for (long long j = (k > NS ? k - NS : 0); j < k; ++j)
+                mbar_wait_bounded(&full[j % NS], (unsigned)((j / NS) & 1), WAIT_LIMIT);
+            if (failed && P.err) atomicExch(P.err, 1);
+        }
+    } else if (warp <= NC) {
+        const int ctid = threadIdx.x - 32;
+        long long k = 0;
+        for (long long r = blockIdx.x; r < nrows; r += gridDim.x, ++k) {
+            const int s = (int)(k % NS);
+            const long long use = k / NS;
+            if (!mbar_wait_bounded(&full[s], (unsigned)(use & 1), WAIT_LIMIT)) {
+                if (lane == 0 && P.err) atomicExch(P.err, 1);
+                break;
+            }
+            const T* st = (const T*)(smem_raw + s * stage_bytes);
+            Geo g;
+            g.y = (int)(r % P.ny);
+            g.z = (int)(r / P.ny);
+            g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+            g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+            g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+            g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+            for (int x0 = 0; x0 < P.nx; x0 += NC * 32) {
+                g.x = x0 + ctid;
+                const bool inside = g.x < P.nx;
+                if (!inside) g.x = 0;
+                g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+                g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+                g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+                g.offsets(P);
+                const uint32_t mk = inside ? P.mask[g.cell] : M_SOLID;
+                const bool active = !(mk & M_SOLID);
+                if (active) {
+                    R f[Q];
+                    auto src = [&](auto I) {
+                        constexpr int i = I;
+                        const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
+                        return st + (i * P.nx + xs);
+                    };
+                    if (__all_sync(__activemask(), !(mk & M_LINKS))) {
+                        sfor<Q>([&](auto I) { f[I] = S::cvt(*src(I)); });
+                    } else {
+                        // branch-free: a generic load from this node's own f*[ibar] in global
+                        // memory (linked direction) or from the staged row in shared memory
+                        sfor<Q>([&](auto I) {
+                            constexpr int i = I, ib = L::qbar(i);
+                            const T* p = ((mk >> ib) & 1u) ? (const T*)P.srcp[ib] + g.cell : src(I);
+                            f[i] = S::cvt(*p);
+                        });
+                    }
+                    process_cell<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc);
+                }
+                constexpr int per = 32 / (int)sizeof(T);
+                const unsigned fl = __ballot_sync(0xffffffffu, active);
+                const unsigned grp = ((1u << per) - 1u) << ((lane / per) * per);
+                if (inside && (mk & M_SOLID) && (fl & grp)) sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+        }
+    }
+    if (P.residual) block_accumulate<5>(racc, P.accum);
 }
 
 }  // namespace lbf

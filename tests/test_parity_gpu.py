@@ -331,17 +331,21 @@ def test_mass_conservation_and_solve_path(Domain):
 
 @pytest.mark.parametrize("storage", [Storage.F64, Storage.F32, Storage.F16DEV])
 def test_staged_and_unstaged_sweeps_agree(Domain, storage):
-    """The bulk-copy staged sweep and the plain-load sweep compute identical results."""
+    """The pipelined, the one-shot staged and the plain-load sweeps compute identical results."""
     mask = cases.sphere_pack([32, 20, 16], 0.75, 2.0, 3.5, seed=13)
     p = cases.porous_channel_d3q19([32, 20, 16], mask=mask, force=1e-5, storage=storage)
     out = []
-    for stage in (1, 0):
+    for pipe, stage in ((1, 0), (0, 1), (0, 0)):
         with Domain(p) as gd:
+            gd.set_option(_abi.LBF_OPT_PIPE, pipe)
             gd.set_option(_abi.LBF_OPT_STAGE, stage)
+            assert gd.get_option(_abi.LBF_OPT_PIPE) == pipe
             assert gd.get_option(_abi.LBF_OPT_STAGE) == stage
-            gd.init().step(60)
-            out.append(gd.moments())
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+            gd.init().step(60, residual_interval=7)
+            out.append(gd.moments() + (gd.residuals()[0],))
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
+        assert np.allclose(out[0][3], o[3], rtol=1e-12, atol=0)
 
 
 @pytest.mark.parametrize("storage,tol", [(Storage.F16DEV, 3e-2), (Storage.BF16DEV, 2e-1)])
