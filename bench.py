@@ -45,23 +45,27 @@ def parse():
     ap.add_argument("--storage", default="f32", choices=list(STORAGE))
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--porosity", type=float, default=0.7, help="target fluid fraction (1.0 = empty channel)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block", type=int, default=0, help="override the x block size")
     ap.add_argument("--sweep", default="plain", choices=["pipe", "stage", "plain"],
                     help="pipelined bulk-copy sweep, one-shot staged sweep, or plain loads")
     ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
+    ap.add_argument("--compact", type=int, default=-1, help="1/0: force the fluid work-list sweep on/off")
     return ap.parse_args()
 
 
-def geometry(n: int, seed: int) -> np.ndarray:
+def geometry(n: int, seed: int, porosity: float = 0.7) -> np.ndarray:
     from lbflow_b200.cases import sphere_pack
+    if porosity >= 1.0:
+        return np.zeros(n ** 3, dtype=np.uint8)
     cache = os.path.join(tempfile.gettempdir(), "lbflow_b200_cache")
     os.makedirs(cache, exist_ok=True)
-    path = os.path.join(cache, f"spheres_{n}_{seed}_p070_r4-10.npy")
+    path = os.path.join(cache, f"spheres_{n}_{seed}_p{int(round(porosity * 100)):03d}_r4-10.npy")
     if os.path.exists(path):
         return np.load(path)
-    mask = sphere_pack([n, n, n], 0.7, 4.0, 10.0, seed)
+    mask = sphere_pack([n, n, n], porosity, 4.0, 10.0, seed)
     np.save(path, mask)
     return mask
 
@@ -74,7 +78,7 @@ def params_for(args, mask):
 
 def workload_name(args):
     return (f"D3Q19 TRT porous channel {args.n}^3 (tau+=0.8, magic 1/4, g_x=1e-6, spheres r in [4,10], "
-            f"porosity 0.7, periodic x, no-slip y/z)")
+            f"porosity {args.porosity:g}, periodic x, no-slip y/z)")
 
 
 class Clocks:
@@ -168,7 +172,7 @@ def cpu_baseline(args, mask, steps=3):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    mask = geometry(args.n, args.seed)
+    mask = geometry(args.n, args.seed, args.porosity)
     from lbflow_b200 import momentum as m
     from oracle import oracle as orc
     p = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
@@ -200,7 +204,7 @@ def run_engine(args, rank, world, local_rank):
     from lbflow_b200.domain import Domain, solve_arrays
 
     torch.cuda.set_device(local_rank)
-    mask = geometry(args.n, args.seed)
+    mask = geometry(args.n, args.seed, args.porosity)
     p = params_for(args, mask)
     n_fluid = int(np.count_nonzero(mask == 0))
     N = mask.size
@@ -212,9 +216,12 @@ def run_engine(args, rank, world, local_rank):
     dom.set_option(_abi.LBF_OPT_STAGE, 1 if args.sweep == "stage" else 0)
     if args.stages:
         dom.set_option(_abi.LBF_OPT_PIPE_STAGES, args.stages)
-    sweep = ("pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
-             "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else "plain loads")
+    if args.compact >= 0:
+        dom.set_option(_abi.LBF_OPT_COMPACT, args.compact)
     dom.init(stream)
+    sweep = ("pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
+             "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else
+             "compacted fluid work list" if dom.get_option(_abi.LBF_OPT_COMPACT) else "dense lattice")
     dom.step(args.warmup, 0, stream)
     torch.cuda.synchronize()
     if world > 1:

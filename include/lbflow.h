@@ -215,8 +215,12 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  * LBF_OPT_PIPE     1 = pipelined bulk-copy sweep on the lean path (faces periodic or
  *                  no-slip, no scalar, rows 16-byte aligned); default 0 (plain loads).
  * LBF_OPT_PIPE_STAGES  ring depth of the pipelined sweep (0 = from the smem budget).
+ * LBF_OPT_COMPACT  1 = on the lean path, sweep a list of the fluid nodes (plus solid
+ *                  nodes sharing a 32-byte sector with them) instead of the dense
+ *                  lattice; default on for FP64 storage only (where it is faster); set
+ *                  before lbf_domain_init.  get: 1 when in effect.
  * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
-enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3 };
+enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */

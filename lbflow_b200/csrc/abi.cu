@@ -14,6 +14,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_select.cuh>
+
 #include "../../include/lbflow.h"
 #include "dispatch.cuh"
 
@@ -159,6 +161,11 @@ struct lbf_domain {
     bool stage = false;           // one-shot staged sweep (off: the pipelined sweep supersedes it)
     bool pipe = false;            // pipelined bulk-copy sweep on the lean path (option)
     int pipe_stages = 0;          // 0 = chosen from the shared-memory budget
+    bool compact = false;         // compacted sweep over a work list on the lean path (in effect)
+    int compact_opt = -1;         // -1 = default (FP64 storage only), 0 off, 1 on
+    uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
+    long long nlist = 0;
+    long long Np = 0;             // population plane stride: N rounded up to 64 nodes
     int* err = nullptr;           // device flag: a bounded wait gave up
     cudaStream_t last_stream = nullptr;
     long long bytes = 0;
@@ -170,7 +177,7 @@ struct lbf_domain {
         }
         for (int f = 0; f < 6; ++f) cudaFree(snap[f]);
         cudaFree(mask); cudaFree(dtype); cudaFree(qads); cudaFree(cprev); cudaFree(c_init_dev);
-        cudaFree(accum); cudaFree(res_dev); cudaFree(obs); cudaFree(counts); cudaFree(err);
+        cudaFree(accum); cudaFree(res_dev); cudaFree(obs); cudaFree(counts); cudaFree(err); cudaFree(list);
         if (res_host) cudaFreeHost(res_host);
     }
     int nfields() const { return 1 + d + (scalar ? 1 : 0); }
@@ -281,6 +288,46 @@ bool face_needs_layers(const lbf_domain* D, int f) {
     return false;
 }
 
+// Work list of the compacted sweep: fluid nodes and the solid nodes that share a
+// 32-byte sector of a population plane with a fluid node, in node order.
+lbf_status build_list(lbf_domain* D, cudaStream_t s) {
+    const long long N = D->N;
+    const int per = (int)(32 / st_bytes(D->st));
+    uint8_t* keep = nullptr;
+    uint32_t* val = nullptr;
+    int* nsel = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    lbf_status st = LBF_OK;
+    cudaError_t e = cudaMalloc(&keep, N);
+    if (e == cudaSuccess) e = cudaMalloc(&val, N * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&nsel, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&D->list, N * 4);
+    if (e == cudaSuccess) {
+        const unsigned nb = (unsigned)((N + 255) / 256);
+        if (D->d == 2) k_list_mark<2><<<nb, 256, 0, s>>>(D->mask, N, (int)D->n[0], (int)D->n[1], (int)D->n[2], per, keep, val);
+        else k_list_mark<3><<<nb, 256, 0, s>>>(D->mask, N, (int)D->n[0], (int)D->n[1], (int)D->n[2], per, keep, val);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, tmp_bytes, val, keep, D->list, nsel, (int)N, s);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(tmp, tmp_bytes, val, keep, D->list, nsel, (int)N, s);
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nsel, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(keep); cudaFree(val); cudaFree(nsel); cudaFree(tmp);
+    if (e != cudaSuccess) {
+        cudaFree(D->list);
+        D->list = nullptr;
+        st = fail(e == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_EDEVICE,
+                  std::string("work list: ") + cudaGetErrorString(e));
+    } else {
+        D->nlist = h;
+        D->bytes += N * 4;
+    }
+    return st;
+}
+
 // Node classification + device masks (Lattice::new), run once before init.
 lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaStream_t s) {
     const long long N = D->N;
@@ -341,6 +388,11 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
             CK(cudaMemsetAsync(D->snap[f], 0, b, s));   // solid neighbours read as zero populations
         }
     }
+    D->nlist = 0;
+    if (D->list) { cudaFree(D->list); D->list = nullptr; }
+    const bool want = D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0;
+    D->compact = want;
+    if (!D->facebc && !D->scalar && want && N < (1ll << 30) && (st = build_list(D, s))) return st;
     D->prepared = true;
     return LBF_OK;
 }
@@ -351,10 +403,14 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.N = D->N;
     P.mask = D->mask;
     P.err = D->err;
+    P.list = D->list;
+    P.nlist = D->nlist;
+    P.inv_nx = 1.0 / (double)D->n[0];
+    P.inv_ny = 1.0 / (double)D->n[1];
     const size_t eb = st_bytes(D->st);
     for (int i = 0; i < D->q; ++i) {
-        P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->N * eb;
-        P.dstp[i] = (char*)D->pop[(t + 1) & 1] + (size_t)i * D->N * eb;
+        P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->Np * eb;
+        P.dstp[i] = (char*)D->pop[(t + 1) & 1] + (size_t)i * D->Np * eb;
     }
     const lbf_collision_desc& c = D->desc.collision;
     P.coll = c.kind; P.compat = D->desc.compat; P.has_force = D->desc.has_force; P.first = t == 0;
@@ -384,8 +440,8 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
         P.c_init = D->c_init_dev;
         const size_t rb = rt_bytes(D->st);
         for (int i = 0; i < D->q; ++i) {
-            P.gsrcp[i] = (const char*)D->gpop[t & 1] + (size_t)i * D->N * rb;
-            P.gdstp[i] = (char*)D->gpop[(t + 1) & 1] + (size_t)i * D->N * rb;
+            P.gsrcp[i] = (const char*)D->gpop[t & 1] + (size_t)i * D->Np * rb;
+            P.gdstp[i] = (char*)D->gpop[(t + 1) & 1] + (size_t)i * D->Np * rb;
         }
         P.qads = D->qads;
         P.cprev = D->cprev;
@@ -439,13 +495,33 @@ cudaError_t launch_pipe(lbf_domain* D, const StepParams& P, cudaStream_t s) {
     }
 }
 
+cudaError_t launch_list(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    const int coll = D->desc.collision.kind;
+    switch (D->vs) {
+        case LBF_D2Q9:
+            return coll == LBF_BGK ? launch_step_list<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, s)
+                 : coll == LBF_TRT ? launch_step_list<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, s)
+                                   : launch_step_list<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, s);
+        case LBF_D3Q19:
+            return coll == LBF_BGK ? launch_step_list<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, s)
+                 : coll == LBF_TRT ? launch_step_list<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, s)
+                                   : launch_step_list<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, s);
+        default:
+            return coll == LBF_BGK ? launch_step_list<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), s)
+                 : coll == LBF_TRT ? launch_step_list<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), s)
+                                   : launch_step_list<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), s);
+    }
+}
+
 // The bulk sweep, then one face pass per scalar outflow face.
 cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
-    if (D->pipe && can_pipe(D) && !P.first && !P.observe && !P.face_pass) {
+    const bool lean = !D->facebc && !D->scalar && !P.first && !P.observe && !P.face_pass;
+    if (D->pipe && lean && can_pipe(D)) {
         cudaError_t e = launch_pipe(D, P, s);
         if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
     }
+    if (lean && D->compact && D->list) return launch_list(D, P, s);
     const bool stage = D->stage && can_stage(D);
     const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
     cudaError_t e = launch_one(D, P, stage, Launch{step_grid(D, b), b, s});
@@ -648,7 +724,8 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
             }
     }
     lbf_status st;
-    const size_t pbytes = (size_t)D->q * N * st_bytes(D->st);
+    D->Np = (N + 63) / 64 * 64;   // every plane starts on a 256-byte boundary
+    const size_t pbytes = (size_t)D->q * D->Np * st_bytes(D->st);
     for (int k = 0; k < 2; ++k)
         if ((st = dmalloc(D, &D->pop[k], pbytes))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->accum, NSLOT * NACC * sizeof(double)))) { delete D; return st; }
@@ -694,7 +771,7 @@ lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
     lbf_status st;
     const size_t rb = rt_bytes(D->st);
     for (int k = 0; k < 2; ++k)
-        if ((st = dmalloc(D, &D->gpop[k], (size_t)D->q * D->N * rb))) return st;
+        if ((st = dmalloc(D, &D->gpop[k], (size_t)D->q * D->Np * rb))) return st;
     if (s->has_adsorption) {
         if ((st = dmalloc(D, &D->qads, D->N * rb))) return st;
         if ((st = dmalloc(D, &D->cprev, D->N * rb))) return st;
@@ -854,6 +931,10 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
             if (value < 0 || value == 1 || value > 16) return fail(LBF_EINVAL, "pipeline stages must be 0 (auto) or 2..16");
             D->pipe_stages = (int)value;
             return LBF_OK;
+        case LBF_OPT_COMPACT:
+            if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_COMPACT before lbf_domain_init");
+            D->compact_opt = value != 0 ? 1 : 0;
+            return LBF_OK;
         default:
             return fail(LBF_EINVAL, "unknown option");
     }
@@ -866,6 +947,7 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
         case LBF_OPT_STAGE: *value = (D->stage && can_stage(D)) ? 1 : 0; return LBF_OK;
         case LBF_OPT_PIPE: *value = (D->pipe && can_pipe(D)) ? 1 : 0; return LBF_OK;
         case LBF_OPT_PIPE_STAGES: *value = D->pipe_stages; return LBF_OK;
+        case LBF_OPT_COMPACT: *value = (D->compact && D->list) ? 1 : 0; return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
     }
 }

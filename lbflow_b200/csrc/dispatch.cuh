@@ -90,6 +90,18 @@ cudaError_t launch_pipe_st(const KParams<VS>& kp, int stages, int nc, cudaStream
     return cudaGetLastError();
 }
 
+// Compacted sweep over the domain's work list (lean path).
+template <int VS, int COLL>
+cudaError_t launch_step_list(int st, const StepParams& base, const double* lam, cudaStream_t stream);
+
+template <int VS, int COLL, int ST>
+cudaError_t launch_list_st(const KParams<VS>& kp, cudaStream_t stream) {
+    const unsigned blocks = (unsigned)((kp.nlist + 255) / 256);
+    if (blocks == 0) return cudaSuccess;
+    k_step_list<VS, COLL, ST><<<blocks, 256, 0, stream>>>(kp);
+    return cudaGetLastError();
+}
+
 // One translation unit per (velocity set, collision) instantiates the step kernels.
 template <int VS, int COLL>
 cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const StepParams& base, const double* lam,
@@ -106,6 +118,20 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
         fill_lam(kp, lam);                                                                             \
         LBF_STEP_COLL(COLL_)                                                                           \
         return cudaErrorInvalidValue;                                                                  \
+    }                                                                                                  \
+    template <>                                                                                        \
+    cudaError_t launch_step_list<VS_, COLL_>(int st, const StepParams& base, const double* lam,         \
+                                             cudaStream_t stream) {                                    \
+        KParams<VS_> kp;                                                                               \
+        static_cast<StepParams&>(kp) = base;                                                           \
+        fill_lam(kp, lam);                                                                             \
+        switch (st) {                                                                                  \
+            case ST_F64: return launch_list_st<VS_, COLL_, ST_F64>(kp, stream);                        \
+            case ST_F32: return launch_list_st<VS_, COLL_, ST_F32>(kp, stream);                        \
+            case ST_F16: return launch_list_st<VS_, COLL_, ST_F16>(kp, stream);                        \
+            case ST_BF16: return launch_list_st<VS_, COLL_, ST_BF16>(kp, stream);                      \
+            default: return cudaErrorInvalidValue;                                                     \
+        }                                                                                              \
     }                                                                                                  \
     template <>                                                                                        \
     cudaError_t launch_step_pipe<VS_, COLL_>(int st, const StepParams& base, const double* lam,         \

@@ -87,6 +87,9 @@ struct StepParams {
     int face_pass, fp_face;   // face pass: update the nodes of face fp_face only
     int* err;                 // set to 1 when a bounded wait gives up
     int pipe_stages, pipe_nc; // pipelined sweep: ring stages, consumer warps
+    const uint32_t* list;     // compacted sweep: work entries (see k_step_list)
+    long long nlist;
+    double inv_nx, inv_ny;    // 1/nx, 1/ny for index -> coordinate conversion
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -1092,6 +1095,100 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         }
     }
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+}
+
+// =================================================================== compacted sweep
+// The hot path of the lean case (periodic / no-slip faces, no scalar, not the
+// first step, not observe).  Threads map to a per-domain list of work entries
+// instead of to the dense lattice: every fluid node, plus every solid node that
+// shares a 32-byte sector of the population planes with a fluid node (those
+// store zeros, so that every store covers whole sectors and needs no DRAM read
+// to fill).  In a porous medium this keeps all lanes busy with fluid work.
+// Entry = node index | (1 << 31) when the node lies on a face of the box (only
+// those need the periodic-wrap offsets; the others use constant ones) | (1 << 30)
+// when the node is solid or has links (only those read the mask word).
+template <int VS, int COLL, int ST>
+__global__ void __launch_bounds__(256, ST == ST_F64 ? 2 : 4) k_step_list(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool valid = t < P.nlist;
+    const uint32_t e = valid ? P.list[t] : 0u;
+    Geo g;
+    g.cell = (int)(e & 0x3fffffffu);
+    if (e >> 31) {
+        // coordinates by a double-precision reciprocal plus a +-1 correction
+        // (exact for indices < 2^31), much cheaper than integer division
+        auto divq = [](int n, int d, double inv) {
+            int q = (int)((double)n * inv);
+            q -= ((long long)q * d > n);
+            q += ((long long)(q + 1) * d <= n);
+            return q;
+        };
+        const int row = divq(g.cell, P.nx, P.inv_nx);
+        g.x = g.cell - row * P.nx;
+        g.z = divq(row, P.ny, P.inv_ny);
+        g.y = row - g.z * P.ny;
+        g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+        g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+        g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+        g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+        g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+        g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+        g.offsets(P);
+    } else {
+        g.oxm = -1;
+        g.oxp = 1;
+        g.oym = -P.nx;
+        g.oyp = P.nx;
+        g.ozm = -P.nx * P.ny;
+        g.ozp = P.nx * P.ny;
+    }
+    // plain fluid entries (no links) need neither the mask word nor any test
+    const bool special = (e >> 30) & 1u;
+    const uint32_t mk = !valid ? M_SOLID : (special ? P.mask[g.cell] : 0u);
+    const bool active = !(mk & M_SOLID);
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (active) {
+        R f[Q];
+        if (__all_sync(__activemask(), !special)) {
+            sfor<Q>([&](auto I) {
+                constexpr int i = I;
+                f[i] = S::ld(P.srcp[i], g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P));
+            });
+        } else {
+            sfor<Q>([&](auto I) {
+                constexpr int i = I, ib = L::qbar(i);
+                const bool lk = (mk >> ib) & 1u;
+                f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i],
+                             lk ? g.cell : g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P));
+            });
+        }
+        process_cell<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc);
+    } else if (valid) {
+        sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
+    }
+    if (P.residual) block_accumulate<5>(racc, P.accum);
+}
+
+// Marks the work entries of the compacted sweep and encodes them (see k_step_list).
+template <int D>
+__global__ void k_list_mark(const uint32_t* mask, long long N, int nx, int ny, int nz, int per, uint8_t* keep,
+                            uint32_t* val) {
+    const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (cell >= N) return;
+    bool k = !(mask[cell] & M_SOLID);
+    if (!k) {
+        const long long s0 = (cell / per) * per;
+        for (long long c = s0; c < s0 + per && c < N; ++c) k = k || !(mask[c] & M_SOLID);
+    }
+    const int x = (int)(cell % nx), y = (int)((cell / nx) % ny), z = (int)(cell / ((long long)nx * ny));
+    const bool edge = x == 0 || x == nx - 1 || y == 0 || y == ny - 1 || (D == 3 && (z == 0 || z == nz - 1));
+    const bool special = (mask[cell] & (M_SOLID | M_LINKS)) != 0;
+    keep[cell] = k ? 1 : 0;
+    val[cell] = (uint32_t)cell | (edge ? 0x80000000u : 0u) | (special ? 0x40000000u : 0u);
 }
 
 // =================================================================== pipelined sweep

@@ -331,14 +331,15 @@ def test_mass_conservation_and_solve_path(Domain):
 
 @pytest.mark.parametrize("storage", [Storage.F64, Storage.F32, Storage.F16DEV])
 def test_staged_and_unstaged_sweeps_agree(Domain, storage):
-    """The pipelined, the one-shot staged and the plain-load sweeps compute identical results."""
+    """The pipelined, one-shot staged, dense and compacted sweeps compute identical results."""
     mask = cases.sphere_pack([32, 20, 16], 0.75, 2.0, 3.5, seed=13)
     p = cases.porous_channel_d3q19([32, 20, 16], mask=mask, force=1e-5, storage=storage)
     out = []
-    for pipe, stage in ((1, 0), (0, 1), (0, 0)):
+    for pipe, stage, compact in ((1, 0, 0), (0, 1, 0), (0, 0, 0), (0, 0, 1)):
         with Domain(p) as gd:
             gd.set_option(_abi.LBF_OPT_PIPE, pipe)
             gd.set_option(_abi.LBF_OPT_STAGE, stage)
+            gd.set_option(_abi.LBF_OPT_COMPACT, compact)
             assert gd.get_option(_abi.LBF_OPT_PIPE) == pipe
             assert gd.get_option(_abi.LBF_OPT_STAGE) == stage
             gd.init().step(60, residual_interval=7)
