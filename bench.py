@@ -39,7 +39,7 @@ SBYTES = {"f64": 8, "f32": 4, "f16dev": 2, "bf16dev": 2}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--storage", default="f32", choices=list(STORAGE))
@@ -79,6 +79,12 @@ def params_for(args, mask):
 def workload_name(args):
     return (f"D3Q19 TRT porous channel {args.n}^3 (tau+=0.8, magic 1/4, g_x=1e-6, spheres r in [4,10], "
             f"porosity {args.porosity:g}, periodic x, no-slip y/z)")
+
+
+def config_of(args, n_fluid, world, sweep):
+    return {"workload": workload_name(args), "storage": args.storage, "n_fluid": int(n_fluid),
+            "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
+            "parallelism": "replicas" if world > 1 else "single", "sweep": sweep}
 
 
 class Clocks:
@@ -153,7 +159,7 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(args, mask, steps=3):
+def cpu_baseline(args, mask, steps=25):
     """The oracle on the full lattice for a few main_steps on all host cores."""
     from lbflow_b200 import momentum as m
     from oracle import oracle as orc
@@ -191,7 +197,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world,
             "steps": k, "warmup": warm, "ms_per_step": dt / k * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sphere packing)",
-            "config": {"workload": workload_name(args), "storage": "f64 (CPU)"},
+            "config": config_of(args, od.num_fluid, world, "CPU oracle, FP64, OpenMP"),
             "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -222,12 +228,13 @@ def run_engine(args, rank, world, local_rank):
     sweep = ("pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
              "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else
              "compacted fluid work list" if dom.get_option(_abi.LBF_OPT_COMPACT) else "dense lattice")
-    dom.step(args.warmup, 0, stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # the clock sampler starts before the warm-up so that its samples cover the timed steps
     with Clocks(local_rank) as clk:
+        dom.step(args.warmup, 0, stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
         start.record(stream)
         dom.step(args.steps, 0, stream)
@@ -279,10 +286,7 @@ def run_engine(args, rank, world, local_rank):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64",
             "data": "synthetic (seeded sphere packing)",
-            "config": {"workload": workload_name(args), "storage": args.storage, "n_fluid": n_fluid,
-                       "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "sweep": sweep},
+            "config": config_of(args, n_fluid, world, sweep),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
