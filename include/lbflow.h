@@ -248,6 +248,23 @@ lbf_status lbf_inventory_noalloc(const double* density, const double* velocity, 
                                  const double* q_ads, const uint32_t* node_class, int64_t n, int32_t d,
                                  double* out, void* stream);
 
+/* ---- output text (the reference's CSV writers) ---------------------------- */
+/* The reference writes every output step as `{:.8e}` CSV text, one node per line
+ * (src/momentum/io.rs:112-192, src/passive_scalar/io.rs:76-108), and the node
+ * coordinates once (src/momentum/io.rs:194-224).  These host-only calls format
+ * that text on `threads` host threads (<= 0: all cores) in Rust's style
+ * ("1.00000000e0", "-2.50000000e-5", "NaN", "inf").  lbf_format_csv writes `rows`
+ * lines of `cols` comma-separated values taken row-major from `values`;
+ * lbf_format_coordinates writes the "i,j[,k],x,y[,z],fluid|solid" rows of an
+ * n[0] x n[1] (x n[2]) lattice with node-centred coordinates (i + 0.5) * delta_x
+ * (src/momentum/lattice.rs:86-89).  Neither writes a header line.  With out ==
+ * NULL they only report the length in *len; otherwise they fail with LBF_EINVAL
+ * if cap < *len. */
+lbf_status lbf_format_csv(const double* values, int64_t rows, int32_t cols, char* out, int64_t cap,
+                          int64_t* len, int32_t threads);
+lbf_status lbf_format_coordinates(const int64_t* n, int32_t d, double delta_x, const uint8_t* node_type,
+                                  char* out, int64_t cap, int64_t* len, int32_t threads);
+
 /* ---- whole solve with host buffers (the `lbflow::solve` drop-in) --------- */
 /* Creates a domain from `desc` (+ optional scalar), initialises it, runs
  * `nsteps` main_steps and copies the final moments to the host arrays.

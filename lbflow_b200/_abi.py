@@ -106,6 +106,8 @@ SIGNATURES = {
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),
     "lbf_inventory_noalloc": (_I32, [_P, _P, _P, _P, _P, _I64, _I32, _P, _P]),
+    "lbf_format_csv": (_I32, [_P, _I64, _I32, _P, _I64, _PI64, _I32]),
+    "lbf_format_coordinates": (_I32, [_PI64, _I32, _D, _P, _P, _I64, _PI64, _I32]),
 }
 
 _LIB_NAME = "liblbflow_b200.so"

@@ -29,9 +29,81 @@ BOUNCE_BACK_MAP_FILE = "map.xyz"
 
 def rust_e8(x: float) -> str:
     """Rust's `{:.8e}` formatting: 8 fraction digits, exponent without padding or '+'."""
+    if x != x:
+        return "NaN"
+    if x in (float("inf"), float("-inf")):
+        return "inf" if x > 0 else "-inf"
     s = f"{x:.8e}"
     mant, exp = s.split("e")
     return f"{mant}e{int(exp)}"
+
+
+# ------------------------------------------------------------------ native text formatting
+def format_rows_native(values: np.ndarray, threads: int = 0) -> memoryview:
+    """`{:.8e}` CSV lines of a (rows, cols) FP64 array, formatted by lbf_format_csv
+    on `threads` host threads (0 = all cores).  Same text as the pure-Python writers."""
+    import ctypes as C
+    from . import _abi
+    lib = _abi.load()
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    rows = v.shape[0]
+    cols = 1 if v.ndim == 1 else v.shape[1]
+    n = C.c_int64()
+    cap = rows * (cols * 25 + 1)
+    buf = np.empty(max(cap, 1), dtype=np.uint8)
+    _abi.check(lib.lbf_format_csv(v.ctypes.data, rows, cols, buf.ctypes.data, cap, C.byref(n), threads))
+    return memoryview(buf)[:n.value]
+
+
+def format_coordinates_native(n: Sequence[int], node_type: Optional[np.ndarray], delta_x: float,
+                              threads: int = 0) -> memoryview:
+    import ctypes as C
+    from . import _abi
+    lib = _abi.load()
+    d = len(n)
+    nn = np.array(list(n) + [1] * (3 - d), dtype=np.int64)
+    rows = int(np.prod(nn))
+    nt = None if node_type is None else np.ascontiguousarray(node_type, dtype=np.uint8)
+    cap = rows * (3 * 21 + 3 * 25 + 8)
+    buf = np.empty(max(cap, 1), dtype=np.uint8)
+    ln = C.c_int64()
+    _abi.check(lib.lbf_format_coordinates(nn.ctypes.data_as(C.POINTER(C.c_int64)), d, float(delta_x), None if nt is None else nt.ctypes.data,
+                                          buf.ctypes.data, cap, C.byref(ln), threads))
+    return memoryview(buf)[:ln.value]
+
+
+def _split_lines(text: memoryview, rows: int, parts: int) -> list:
+    """Byte ranges of `parts` chunks of rows_per = rows // parts lines (the last ones
+    may be shorter), matching rayon's par_chunks(rows / parts)."""
+    if parts <= 1 or rows == 0:
+        return [text]
+    chunk = max(1, rows // parts)
+    a = np.frombuffer(text, dtype=np.uint8)
+    ends = np.flatnonzero(a == 10) + 1          # end offset of every line
+    out, start = [], 0
+    for r0 in range(0, rows, chunk):
+        r1 = min(rows, r0 + chunk)
+        stop = int(ends[r1 - 1])
+        out.append(text[start:stop])
+        start = stop
+    return out
+
+
+def write_field_native(step_path: str, prefix: str, header: str, values: np.ndarray, num_threads: int = 1,
+                       format_threads: int = 0) -> None:
+    """One field of an output step, as _write_chunks writes it, with native formatting."""
+    text = format_rows_native(values, format_threads)
+    rows = values.shape[0]
+    parts = _split_lines(text, rows, num_threads)
+    if num_threads <= 1:
+        with open(os.path.join(step_path, f"{prefix}.csv"), "wb") as fh:
+            fh.write((header + "\n").encode())
+            fh.write(text)
+        return
+    for i, part in enumerate(parts):
+        with open(os.path.join(step_path, f"{prefix}_{i}.csv"), "wb") as fh:
+            fh.write((header + "\n").encode())
+            fh.write(part)
 
 
 def format_column(values: np.ndarray) -> list:
