@@ -53,6 +53,13 @@ def parse():
                     help="pipelined bulk-copy sweep, one-shot staged sweep, or plain loads")
     ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
     ap.add_argument("--compact", type=int, default=-1, help="1/0: force the fluid work-list sweep on/off")
+    ap.add_argument("--workload", default="step", choices=["step", "serve"],
+                    help="step: the fused step on one lattice (headline); serve: the serving mix")
+    ap.add_argument("--requests", type=int, default=300, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=float("inf"), help="serve: Poisson arrivals per second (inf = all at t=0)")
+    ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
+    ap.add_argument("--chunk", type=int, default=50, help="serve: residual interval (steps per chunk)")
+    ap.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time baseline")
     return ap.parse_args()
 
 
@@ -294,6 +301,47 @@ def run_engine(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args, rank, world, local_rank):
+    """The serving mix through one Batch, and one solve at a time as the baseline."""
+    import torch
+    from lbflow_b200 import serve
+    torch.cuda.set_device(local_rank)
+    reqs = serve.make_requests(args.requests, args.rate, args.seed + rank)
+    serve.prepare(reqs)
+    warm = serve.make_requests(6, float("inf"), args.seed + 999)
+    serve.prepare(warm)
+    serve.serve_batched(warm, max_steps=200, residual_interval=args.chunk)
+    serve.serve_sequential(warm, max_steps=200, residual_interval=args.chunk)
+    torch.cuda.synchronize()
+    with Clocks(local_rank) as clk:
+        rb = serve.serve_batched(reqs, max_steps=args.max_steps, residual_interval=args.chunk)
+    sb = serve.summary(rb)
+    ss = None
+    if not args.no_sequential:
+        ss = serve.summary(serve.serve_sequential(reqs, max_steps=args.max_steps, residual_interval=args.chunk))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([sb["seconds"]], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sb["seconds"] = float(t.item())
+    if rank != 0:
+        return
+    line = {"metric": "solves/s", "value": world * sb["solves"] / sb["seconds"], "unit": "solves/s", "n_gpus": world,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded serving mix)",
+            "config": {"workload": f"serving mix: {args.requests} requests, arrivals "
+                                   f"{'all at t=0' if args.rate == float('inf') else f'Poisson {args.rate:g}/s'}, "
+                                   "50% D2Q9 BGK cavities side log-U[64,1024], 50% D3Q19 TRT porous channels side "
+                                   "log-U[32,160] porosity U[0.5,0.9], FP32 / FP16-deviation storage 50/50, "
+                                   f"stop at {args.max_steps} steps or velocity residual < 1e-6 "
+                                   f"(checked every {args.chunk} steps)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "batched": sb, "sequential": ss, "clocks": clk.summary()}
+    if ss:
+        line["speedup_vs_sequential"] = sb["solves_per_s"] / ss["solves_per_s"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -306,6 +354,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "serve":
+        run_serve(args, rank, world, local_rank)
     else:
         run_engine(args, rank, world, local_rank)
         if world > 1:

@@ -265,6 +265,40 @@ lbf_status lbf_format_csv(const double* values, int64_t rows, int32_t cols, char
 lbf_status lbf_format_coordinates(const int64_t* n, int32_t d, double delta_x, const uint8_t* node_type,
                                   char* out, int64_t cap, int64_t* len, int32_t threads);
 
+/* ---- batches: many domains stepped together (serving) --------------------- */
+/* No counterpart in the reference, which solves one case per process.  A batch
+ * advances many initialised domains together: the domains of one kernel
+ * configuration (velocity set, collision, storage, explicit faces) share one
+ * launch per time step, and a chunk of `residual_interval` = k steps plus an
+ * on-device residual + stop-rule evaluation is captured once as a CUDA graph and
+ * replayed.  Each domain stops exactly where lbf_domain_run(max_iterations, k,
+ * tol_*) would stop it, with the same fields.  Domains with a scalar are not
+ * batched (LBF_EUNSUPPORTED).  While admitted, a domain refuses the standalone
+ * calls (LBF_ESTATE); lbf_batch_poll hands it back once it stopped, and
+ * lbf_domain_destroy evicts it first.  The batch object is thread-safe.
+ *
+ * lbf_batch_create: budget_bytes = device bytes the admitted domains may hold
+ *   (0: 90 % of the free device memory now).
+ * lbf_batch_admit: LBF_ENOMEM when the domain's device bytes do not fit the budget.
+ * lbf_batch_step: enqueues nchunks chunks on `stream` (asynchronous).
+ * lbf_batch_poll: returns up to `cap` stopped domains with their status
+ *   (1 converged, 2 max_iterations, 3 non-finite residual); wait = 0 returns
+ *   nothing while the last chunk is still running.
+ * lbf_domain_estimate_bytes: an upper bound of the device bytes a domain built
+ *   from these descriptors holds after init and a moments read (admission control
+ *   before any allocation). */
+typedef struct lbf_batch lbf_batch;
+lbf_status lbf_domain_estimate_bytes(const lbf_domain_desc* desc, const lbf_scalar_desc* scalar, int64_t* bytes);
+lbf_status lbf_batch_create(int64_t budget_bytes, int64_t residual_interval, lbf_batch** out);
+lbf_status lbf_batch_admit(lbf_batch* batch, lbf_domain* dom, int64_t max_iterations, double tol_density,
+                           double tol_velocity, double tol_scalar);
+lbf_status lbf_batch_step(lbf_batch* batch, int64_t nchunks, void* stream);
+lbf_status lbf_batch_poll(lbf_batch* batch, lbf_domain** done, int32_t* status, int32_t cap, int32_t* ndone,
+                          int32_t wait);
+lbf_status lbf_batch_evict(lbf_batch* batch, lbf_domain* dom);
+lbf_status lbf_batch_info(lbf_batch* batch, int64_t* running, int64_t* finished, int64_t* bytes, int64_t* budget);
+lbf_status lbf_batch_destroy(lbf_batch* batch);
+
 /* ---- whole solve with host buffers (the `lbflow::solve` drop-in) --------- */
 /* Creates a domain from `desc` (+ optional scalar), initialises it, runs
  * `nsteps` main_steps and copies the final moments to the host arrays.

@@ -106,6 +106,14 @@ SIGNATURES = {
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),
     "lbf_inventory_noalloc": (_I32, [_P, _P, _P, _P, _P, _I64, _I32, _P, _P]),
+    "lbf_domain_estimate_bytes": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _PI64]),
+    "lbf_batch_create": (_I32, [_I64, _I64, C.POINTER(_P)]),
+    "lbf_batch_admit": (_I32, [_P, _P, _I64, _D, _D, _D]),
+    "lbf_batch_step": (_I32, [_P, _I64, _P]),
+    "lbf_batch_poll": (_I32, [_P, C.POINTER(_P), _PI32, _I32, _PI32, _I32]),
+    "lbf_batch_evict": (_I32, [_P, _P]),
+    "lbf_batch_info": (_I32, [_P, _PI64, _PI64, _PI64, _PI64]),
+    "lbf_batch_destroy": (_I32, [_P]),
     "lbf_format_csv": (_I32, [_P, _I64, _I32, _P, _I64, _PI64, _I32]),
     "lbf_format_coordinates": (_I32, [_PI64, _I32, _D, _P, _P, _I64, _PI64, _I32]),
 }

@@ -17,6 +17,7 @@
 #include <cub/device/device_select.cuh>
 
 #include "../../include/lbflow.h"
+#include "batch.cuh"
 #include "dispatch.cuh"
 
 using namespace lbf;
@@ -42,6 +43,92 @@ int vs_q(int vs) { return vs == LBF_D2Q9 ? 9 : (vs == LBF_D3Q19 ? 19 : (vs == LB
 int vs_d(int vs) { return vs == LBF_D2Q9 ? 2 : 3; }
 size_t st_bytes(int st) { return st == LBF_STORE_F64 ? 8 : (st == LBF_STORE_F32 ? 4 : 2); }
 size_t rt_bytes(int st) { return st == LBF_STORE_F64 ? 8 : 4; }   // compute type
+
+// ---- device and pinned memory --------------------------------------------------
+// Serving creates and destroys domains continuously.  cudaMalloc / cudaFree (and
+// cudaFreeHost) synchronise the whole device and return memory to the driver
+// each time, tens of milliseconds per domain on a busy GPU.  The library
+// therefore allocates device memory from its own stream-ordered pool per device
+// with an unlimited release threshold (freed blocks stay cached for the next
+// domain), on a private non-blocking stream: an allocation waits for that stream
+// only and is then ready for any stream.  A free must come after the last work
+// that uses the memory: lbf_domain_destroy first waits for the domain's last stream.
+constexpr int MAX_DEV = 64;
+struct DevPool {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t s = nullptr;
+};
+std::mutex g_pool_mu;
+DevPool g_pools[MAX_DEV];
+
+cudaError_t pool_of(int dev, DevPool** out) {
+    if (dev < 0 || dev >= MAX_DEV) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    DevPool& P = g_pools[dev];
+    if (!P.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaError_t e = cudaMemPoolCreate(&P.pool, &props);
+        if (e != cudaSuccess) { P.pool = nullptr; return e; }
+        unsigned long long thr = ~0ull;
+        e = cudaMemPoolSetAttribute(P.pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&P.s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(P.pool);
+            P.pool = nullptr;
+            return e;
+        }
+    }
+    *out = &P;
+    return cudaSuccess;
+}
+
+int current_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+cudaError_t dev_alloc(void** p, size_t bytes, int dev) {
+    *p = nullptr;
+    DevPool* P = nullptr;
+    cudaError_t e = pool_of(dev, &P);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, P->pool, P->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(P->s);
+    if (e != cudaSuccess) *p = nullptr;
+    return e;
+}
+
+void dev_free(void* p, int dev) {
+    if (!p) return;
+    DevPool* P = nullptr;
+    if (pool_of(dev, &P) == cudaSuccess) cudaFreeAsync(p, P->s);
+}
+
+// Pinned 64-byte slots (residual read-backs) carved from 4 KiB pinned pages that
+// are never released, so that no cudaFreeHost runs while serving.
+std::mutex g_pin_mu;
+std::vector<void*> g_pin_free;
+
+void* pinned64() {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    if (g_pin_free.empty()) {
+        void* page = nullptr;
+        if (cudaMallocHost(&page, 4096) != cudaSuccess) return nullptr;
+        for (int i = 0; i < 64; ++i) g_pin_free.push_back((char*)page + 64 * i);
+    }
+    void* p = g_pin_free.back();
+    g_pin_free.pop_back();
+    return p;
+}
+
+void pinned64_free(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_free.push_back(p);
+}
 
 // ---- D3Q27 orthogonal moment basis (no reference counterpart: the reference's
 // D3Q27 MRT is a placeholder, src/velocity_set/d3q27.rs:86 and
@@ -122,6 +209,7 @@ void tables_of(int* d, int* q, int* c, double* w, int* qbar, int* qfaces, int* n
 }  // namespace
 
 // ============================================================== the domain
+struct lbf_batch;
 struct lbf_domain {
     lbf_domain_desc desc{};
     int vs = 0, q = 0, d = 0, st = 0, nfaces = 0;
@@ -169,16 +257,19 @@ struct lbf_domain {
     int* err = nullptr;           // device flag: a bounded wait gave up
     cudaStream_t last_stream = nullptr;
     long long bytes = 0;
+    lbf_batch* batch = nullptr;   // set while the domain is admitted to a batch
+    int dev = 0;                  // device that holds the domain's memory
 
     ~lbf_domain() {
         for (int k = 0; k < 2; ++k) {
-            cudaFree(pop[k]); cudaFree(gpop[k]); cudaFree(mom[k]);
-            for (int f = 0; f < 6; ++f) cudaFree(pb[f][k]);
+            dev_free(pop[k], dev); dev_free(gpop[k], dev); dev_free(mom[k], dev);
+            for (int f = 0; f < 6; ++f) dev_free(pb[f][k], dev);
         }
-        for (int f = 0; f < 6; ++f) cudaFree(snap[f]);
-        cudaFree(mask); cudaFree(dtype); cudaFree(qads); cudaFree(cprev); cudaFree(c_init_dev);
-        cudaFree(accum); cudaFree(res_dev); cudaFree(obs); cudaFree(counts); cudaFree(err); cudaFree(list);
-        if (res_host) cudaFreeHost(res_host);
+        for (int f = 0; f < 6; ++f) dev_free(snap[f], dev);
+        for (void* p : {(void*)mask, (void*)dtype, qads, cprev, (void*)c_init_dev, (void*)accum, (void*)res_dev,
+                        (void*)obs, (void*)counts, (void*)err, (void*)list})
+            dev_free(p, dev);
+        pinned64_free(res_host);
     }
     int nfields() const { return 1 + d + (scalar ? 1 : 0); }
 };
@@ -186,12 +277,12 @@ struct lbf_domain {
 namespace {
 
 lbf_status dmalloc(lbf_domain* D, void** p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = dev_alloc(p, bytes, D->dev);
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
         return fail(e == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_EDEVICE,
-                    std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+                    std::string("device allocation (") + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
     }
     D->bytes += (long long)bytes;
     return LBF_OK;
@@ -299,10 +390,10 @@ lbf_status build_list(lbf_domain* D, cudaStream_t s) {
     void* tmp = nullptr;
     size_t tmp_bytes = 0;
     lbf_status st = LBF_OK;
-    cudaError_t e = cudaMalloc(&keep, N);
-    if (e == cudaSuccess) e = cudaMalloc(&val, N * 4);
-    if (e == cudaSuccess) e = cudaMalloc(&nsel, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&D->list, N * 4);
+    cudaError_t e = dev_alloc((void**)&keep, N, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&val, N * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&nsel, sizeof(int), D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&D->list, N * 4, D->dev);
     if (e == cudaSuccess) {
         const unsigned nb = (unsigned)((N + 255) / 256);
         if (D->d == 2) k_list_mark<2><<<nb, 256, 0, s>>>(D->mask, N, (int)D->n[0], (int)D->n[1], (int)D->n[2], per, keep, val);
@@ -310,14 +401,14 @@ lbf_status build_list(lbf_domain* D, cudaStream_t s) {
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, tmp_bytes, val, keep, D->list, nsel, (int)N, s);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+    if (e == cudaSuccess) e = dev_alloc(&tmp, tmp_bytes, D->dev);
     if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(tmp, tmp_bytes, val, keep, D->list, nsel, (int)N, s);
     int h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nsel, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(keep); cudaFree(val); cudaFree(nsel); cudaFree(tmp);
+    dev_free(keep, D->dev); dev_free(val, D->dev); dev_free(nsel, D->dev); dev_free(tmp, D->dev);
     if (e != cudaSuccess) {
-        cudaFree(D->list);
+        dev_free(D->list, D->dev);
         D->list = nullptr;
         st = fail(e == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_EDEVICE,
                   std::string("work list: ") + cudaGetErrorString(e));
@@ -350,10 +441,10 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     lbf_status st;
     if (!D->mask && (st = dmalloc(D, (void**)&D->mask, N * 4))) return st;
     if ((st = dmalloc(D, (void**)&cls, N * 4))) return st;
-    if ((st = dmalloc(D, (void**)&links, N * 4))) { cudaFree(cls); return st; }
+    if ((st = dmalloc(D, (void**)&links, N * 4))) { dev_free(cls, D->dev); return st; }
     D->bytes -= 8 * N;
-    if (!D->counts && (st = dmalloc(D, (void**)&D->counts, 16))) { cudaFree(cls); cudaFree(links); return st; }
-    if (!D->dtype && (st = dmalloc(D, (void**)&D->dtype, N))) { cudaFree(cls); cudaFree(links); return st; }
+    if (!D->counts && (st = dmalloc(D, (void**)&D->counts, 16))) { dev_free(cls, D->dev); dev_free(links, D->dev); return st; }
+    if (!D->dtype && (st = dmalloc(D, (void**)&D->dtype, N))) { dev_free(cls, D->dev); dev_free(links, D->dev); return st; }
     cudaError_t e = cudaMemcpyAsync(D->dtype, D->type.data(), N, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(D->counts, 0, 16, s);
     SetupParams S{};
@@ -370,8 +461,8 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     if (e == cudaSuccess && cls_out) e = cudaMemcpyAsync(cls_out, cls, N * 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && links_out) e = cudaMemcpyAsync(links_out, links, N * 4, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(cls);
-    cudaFree(links);
+    dev_free(cls, D->dev);
+    dev_free(links, D->dev);
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("node classification: ") + cudaGetErrorString(e));
     D->n_fluid = cnt[0];
     D->n_bb = cnt[1];
@@ -389,7 +480,7 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
         }
     }
     D->nlist = 0;
-    if (D->list) { cudaFree(D->list); D->list = nullptr; }
+    if (D->list) { dev_free(D->list, D->dev); D->list = nullptr; }
     const bool want = D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0;
     D->compact = want;
     if (!D->facebc && !D->scalar && want && N < (1ll << 30) && (st = build_list(D, s))) return st;
@@ -568,7 +659,7 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     const size_t nr = D->rho0.empty() ? 0 : D->N, nu = D->u0.empty() ? 0 : D->N * D->d;
     const size_t nc = D->c0.empty() ? 0 : D->N;
     if (nr + nu + nc) {
-        CK(cudaMalloc(&tmp, (nr + nu + nc) * sizeof(double)));
+        CK(dev_alloc((void**)&tmp, (nr + nu + nc) * sizeof(double), D->dev));
         if (nr) CK(cudaMemcpyAsync(tmp, D->rho0.data(), nr * 8, cudaMemcpyHostToDevice, s));
         if (nu) CK(cudaMemcpyAsync(tmp + nr, D->u0.data(), nu * 8, cudaMemcpyHostToDevice, s));
         if (nc) CK(cudaMemcpyAsync(tmp + nr + nu, D->c0.data(), nc * 8, cudaMemcpyHostToDevice, s));
@@ -584,7 +675,7 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
                                        : launch_init<VS_D3Q27>(D->st, D->scalar, P, I, pb, L);
     if (tmp) {
         cudaStreamSynchronize(s);
-        cudaFree(tmp);
+        dev_free(tmp, D->dev);
     }
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("init kernel: ") + cudaGetErrorString(e));
     CK(cudaMemsetAsync(D->accum, 0, NSLOT * NACC * sizeof(double), s));
@@ -699,6 +790,7 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
         }
     }
     lbf_domain* D = new lbf_domain();
+    D->dev = current_device();
     D->desc = *ds;
     D->desc.node_type = nullptr;
     D->desc.initial_density_field = nullptr;
@@ -732,7 +824,7 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     if ((st = dmalloc(D, (void**)&D->res_dev, 8 * sizeof(double)))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->err, sizeof(int)))) { delete D; return st; }
     if (cudaMemset(D->err, 0, sizeof(int)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
-    if (cudaMallocHost(&D->res_host, 8 * sizeof(double)) != cudaSuccess) { delete D; return fail(LBF_ENOMEM, "pinned alloc"); }
+    if (!(D->res_host = (double*)pinned64())) { delete D; return fail(LBF_ENOMEM, "pinned alloc"); }
     std::memset(D->res_host, 0, 8 * sizeof(double));
     if (cudaMemset(D->accum, 0, NSLOT * NACC * sizeof(double)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
     *out = D;
@@ -786,11 +878,13 @@ lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
 
 lbf_status lbf_domain_init(lbf_domain* D, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     return do_init(D, (cudaStream_t)stream);
 }
 
 lbf_status lbf_domain_step(lbf_domain* D, int64_t nsteps, int64_t residual_interval, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     if (nsteps < 0) return fail(LBF_EINVAL, "nsteps < 0");
     return do_steps(D, nsteps, residual_interval, (cudaStream_t)stream);
 }
@@ -798,6 +892,7 @@ lbf_status lbf_domain_step(lbf_domain* D, int64_t nsteps, int64_t residual_inter
 lbf_status lbf_domain_run(lbf_domain* D, int64_t max_iterations, int64_t k, double tr, double tu, double tc,
                           int64_t* steps_done, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     if (k < 1) k = 1;
     cudaStream_t s = (cudaStream_t)stream;
     lbf_status st;
@@ -833,6 +928,7 @@ lbf_status lbf_domain_residuals(lbf_domain* D, double* out, int64_t* time_step) 
 
 lbf_status lbf_domain_get_moments(lbf_domain* D, double* rho, double* u, double* c, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     cudaStream_t s = (cudaStream_t)stream;
     lbf_status st;
     if ((st = do_observe(D, s))) return st;
@@ -871,6 +967,7 @@ lbf_status lbf_domain_get_q_ads(lbf_domain* D, double* q) {
 
 lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     if (!D || !out) return fail(LBF_EINVAL, "null argument");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     cudaStream_t s = (cudaStream_t)stream;
     lbf_status st;
     if ((st = do_observe(D, s))) return st;
@@ -886,12 +983,12 @@ lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     }
     CK(cudaGetLastError());
     double* tmp = nullptr;
-    CK(cudaMalloc(&tmp, 8 * sizeof(double)));
+    CK(dev_alloc((void**)&tmp, 8 * sizeof(double), D->dev));
     k_finalize<<<1, 32, 0, s>>>(D->accum, 6, 0, tmp);
     double h[8];
     cudaError_t e = cudaMemcpyAsync(h, tmp, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    cudaFree(tmp);
+    dev_free(tmp, D->dev);
     if (e != cudaSuccess) return fail(LBF_EDEVICE, cudaGetErrorString(e));
     for (int k = 0; k < 3 + D->d; ++k) out[k] = h[k];
     return LBF_OK;
@@ -954,6 +1051,7 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
 
 lbf_status lbf_domain_destroy(lbf_domain* D) {
     if (D) {
+        if (D->batch) lbf_batch_evict(D->batch, D);
         if (D->last_stream) cudaStreamSynchronize(D->last_stream);
         delete D;
     }
@@ -972,6 +1070,439 @@ lbf_status lbf_solve(const lbf_domain_desc* desc, const lbf_scalar_desc* sdesc, 
         return st;
     }
     return lbf_domain_destroy(D);
+}
+
+}  // extern "C"
+
+// ============================================================== batches
+// A batch advances many initialised domains together: the domains of each kernel
+// configuration (velocity set, collision, storage, explicit faces) form a group,
+// and one launch per group and time step covers all of them (k_step_batch).  A
+// chunk is k time steps (k = residual interval) followed by one finalize launch
+// per group that evaluates each domain's residuals and stop rule on the device;
+// the chunk is captured once as a CUDA graph and replayed until the membership
+// changes.  Every domain joins in phase: its next time step t has
+// t % k == 1 % k, so that the last step of every chunk is its residual step and
+// it stops exactly where lbf_domain_run(max_iterations, k) would.
+struct lbf_batch {
+    struct Member {
+        lbf_domain* D;
+        long long max_it;
+        double tol[3];
+    };
+    struct Group {
+        int vs = 0, coll = 0, st = 0;
+        bool facebc = false;
+        std::vector<int> mem;          // indices into members
+        void* tab = nullptr;           // KParams<vs>[n] (device)
+        BatchState* bs = nullptr;      // device state
+        BatchState* host = nullptr;    // pinned mirror, copied at the end of every chunk
+        int* blk = nullptr;            // block -> position in the group
+        unsigned nblocks = 0;
+    };
+    std::mutex mu;
+    int k = 1;
+    long long budget = 0, bytes = 0;
+    std::vector<Member> members;
+    std::vector<std::pair<lbf_domain*, int>> finished;   // (domain, status) not yet polled
+    std::vector<std::pair<lbf_domain*, long long>> admitted;   // device bytes counted at admission
+    std::vector<Group> groups;
+    bool dirty = true;
+    cudaStream_t cap = nullptr;        // private stream the chunk graph is captured on
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaStream_t last = nullptr;
+    bool launched = false;
+    int dev = 0;
+    BatchState* host_buf = nullptr;   // pinned, grows only (no cudaFreeHost while serving)
+    size_t host_cap = 0;
+
+    void free_groups() {
+        for (auto& g : groups) {
+            dev_free(g.tab, dev); dev_free(g.bs, dev); dev_free(g.blk, dev);
+        }
+        groups.clear();
+        if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    }
+    ~lbf_batch() {
+        if (launched) cudaEventSynchronize(ev);   // the null stream is a valid stream: sync on the event
+        free_groups();
+        if (host_buf) cudaFreeHost(host_buf);
+        if (ev) cudaEventDestroy(ev);
+        if (cap) cudaStreamDestroy(cap);
+    }
+};
+
+namespace {
+
+// Releases the budget share of a domain that leaves the batch.
+void batch_release(lbf_batch* b, lbf_domain* D) {
+    for (size_t i = 0; i < b->admitted.size(); ++i)
+        if (b->admitted[i].first == D) {
+            b->bytes -= b->admitted[i].second;
+            b->admitted.erase(b->admitted.begin() + i);
+            break;
+        }
+    D->batch = nullptr;
+}
+
+size_t kparams_size(int vs) {
+    return vs == LBF_D2Q9 ? sizeof(KParams<VS_D2Q9>)
+         : vs == LBF_D3Q19 ? sizeof(KParams<VS_D3Q19>) : sizeof(KParams<VS_D3Q27>);
+}
+
+// The domain's step parameters laid out for an even time step (t = 0 layout).
+void fill_kparams(const lbf_domain* D, unsigned char* dst) {
+    StepParams P;
+    base_params(D, P, 0);
+    P.first = 0;
+    if (D->vs == LBF_D3Q27) {
+        KParams<VS_D3Q27>* kp = new KParams<VS_D3Q27>();
+        static_cast<StepParams&>(*kp) = P;
+        fill_lam(*kp, D->lam.empty() ? nullptr : D->lam.data());
+        std::memcpy(dst, kp, sizeof(*kp));
+        delete kp;
+    } else {
+        std::memcpy(dst, &P, sizeof(StepParams));   // KParams<VS> adds nothing for D2Q9 / D3Q19
+    }
+}
+
+// Reads the device state of every member (as of the last completed chunk) into
+// the domains: time step, residuals; members that stopped move to `finished`.
+void batch_harvest(lbf_batch* b) {
+    std::vector<bool> gone(b->members.size(), false);
+    for (auto& g : b->groups) {
+        for (size_t p = 0; p < g.mem.size(); ++p) {
+            const int mi = g.mem[p];
+            if (mi < 0 || gone[mi]) continue;
+            lbf_domain* D = b->members[mi].D;
+            const BatchState& s = g.host[p];
+            D->t = s.done_t >= 0 ? s.done_t + 1 : s.t0;
+            if (s.res_t >= 0) {
+                for (int i = 0; i < 5; ++i) D->res_host[i] = s.res[i];
+                D->res_step = s.res_t;
+            }
+            D->last_stream = b->last;
+            if (s.done_t >= 0) {
+                b->finished.emplace_back(D, s.status);
+                gone[mi] = true;
+                g.mem[p] = -1;
+            }
+        }
+    }
+    std::vector<int> remap(b->members.size(), -1);
+    std::vector<lbf_batch::Member> keep;
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        if (gone[i]) continue;
+        remap[i] = (int)keep.size();
+        keep.push_back(b->members[i]);
+    }
+    if (keep.size() != b->members.size()) b->dirty = true;
+    for (auto& g : b->groups)
+        for (auto& m : g.mem) m = m >= 0 ? remap[m] : -1;
+    b->members.swap(keep);
+}
+
+// Single steps (standalone path) until the domain's next step t has t % k == 1 % k.
+// *stopped = the stop status if the rule of lbf_domain_run ended it meanwhile.
+lbf_status phase_align(lbf_domain* D, const lbf_batch::Member& m, int k, cudaStream_t s, int* stopped) {
+    *stopped = 0;
+    while (D->t % k != 1 % k) {
+        const long long t = D->t;
+        lbf_status st = do_steps(D, 1, k, s);
+        if (st) return st;
+        if (t > m.max_it) { *stopped = 2; break; }
+        if (t > 10 && D->res_step == t) {
+            CK(cudaStreamSynchronize(s));
+            if (!std::isfinite(D->res_host[0])) { *stopped = 3; break; }
+            bool conv = D->res_host[0] <= m.tol[0];
+            for (int a = 0; a < D->d; ++a) conv = conv && D->res_host[1 + a] <= m.tol[1];
+            if (conv) { *stopped = 1; break; }
+        }
+    }
+    return LBF_OK;
+}
+
+cudaError_t batch_launch_step(const lbf_batch::Group& g, int j, cudaStream_t s) {
+    switch (g.vs) {
+        case LBF_D2Q9: return launch_step_batch<VS_D2Q9>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
+        case LBF_D3Q19: return launch_step_batch<VS_D3Q19>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
+        default: return launch_step_batch<VS_D3Q27>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
+    }
+}
+cudaError_t batch_launch_finalize(const lbf_batch::Group& g, cudaStream_t s) {
+    const int n = (int)g.mem.size();
+    switch (g.vs) {
+        case LBF_D2Q9: return launch_batch_finalize<VS_D2Q9>(g.tab, g.bs, n, s);
+        case LBF_D3Q19: return launch_batch_finalize<VS_D3Q19>(g.tab, g.bs, n, s);
+        default: return launch_batch_finalize<VS_D3Q27>(g.tab, g.bs, n, s);
+    }
+}
+
+// New groups, device tables and chunk graph for the current members.
+lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
+    if (b->launched) CK(cudaEventSynchronize(b->ev));
+    if (b->launched) batch_harvest(b);
+    b->launched = false;
+    b->free_groups();
+    // phase alignment (may finish some members)
+    std::vector<lbf_batch::Member> keep;
+    for (auto& m : b->members) {
+        int stopped = 0;
+        lbf_status st = phase_align(m.D, m, b->k, s, &stopped);
+        if (st) return st;
+        if (stopped) b->finished.emplace_back(m.D, stopped);
+        else keep.push_back(m);
+    }
+    b->members.swap(keep);
+    CK(cudaStreamSynchronize(s));
+    b->last = s;
+    // groups by kernel configuration
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        const lbf_domain* D = b->members[i].D;
+        const int coll = D->desc.collision.kind;
+        lbf_batch::Group* g = nullptr;
+        for (auto& x : b->groups)
+            if (x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc) g = &x;
+        if (!g) {
+            b->groups.emplace_back();
+            g = &b->groups.back();
+            g->vs = D->vs; g->coll = coll; g->st = D->st; g->facebc = D->facebc;
+        }
+        g->mem.push_back((int)i);
+    }
+    size_t total = 0;
+    for (auto& g : b->groups) total += g.mem.size();
+    if (total > b->host_cap) {
+        const size_t cap = std::max<size_t>(total, 2 * b->host_cap + 64);
+        if (b->host_buf) cudaFreeHost(b->host_buf);
+        b->host_buf = nullptr;
+        b->host_cap = 0;
+        CK(cudaMallocHost((void**)&b->host_buf, cap * sizeof(BatchState)));
+        b->host_cap = cap;
+    }
+    size_t host_off = 0;
+    for (auto& g : b->groups) {
+        const size_t n = g.mem.size(), ks = kparams_size(g.vs);
+        std::vector<unsigned char> tab(n * ks);
+        std::vector<BatchState> bs(n);
+        std::vector<int> blk;
+        for (size_t p = 0; p < n; ++p) {
+            const lbf_batch::Member& m = b->members[g.mem[p]];
+            const lbf_domain* D = m.D;
+            fill_kparams(D, tab.data() + p * ks);
+            BatchState& x = bs[p];
+            std::memset(&x, 0, sizeof(x));
+            x.t0 = D->t;
+            x.last_t = m.max_it + 1;
+            x.block0 = (long long)blk.size();
+            x.done_t = -1;
+            x.res_t = D->res_step;
+            for (int i = 0; i < 5; ++i) x.res[i] = D->res_host[i];
+            x.k = b->k;
+            x.d = D->d;
+            x.has_scalar = D->scalar ? 1 : 0;
+            for (int i = 0; i < 3; ++i) x.tol[i] = m.tol[i];
+            const long long nb = (D->N + BATCH_BLOCK - 1) / BATCH_BLOCK;
+            blk.insert(blk.end(), (size_t)nb, (int)p);
+        }
+        if (blk.size() >= (1ull << 31)) return fail(LBF_EUNSUPPORTED, "batch group larger than 2^31 blocks");
+        g.nblocks = (unsigned)blk.size();
+        CK(dev_alloc(&g.tab, tab.size(), b->dev));
+        CK(dev_alloc((void**)&g.bs, n * sizeof(BatchState), b->dev));
+        CK(dev_alloc((void**)&g.blk, blk.size() * sizeof(int), b->dev));
+        g.host = b->host_buf + host_off;
+        host_off += n;
+        std::memcpy(g.host, bs.data(), n * sizeof(BatchState));
+        CK(cudaMemcpy(g.tab, tab.data(), tab.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(g.bs, bs.data(), n * sizeof(BatchState), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(g.blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    // capture one chunk: k steps of every group, finalize, copy the states back
+    if (!b->members.empty()) {
+        CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int j = 0; j < b->k && e == cudaSuccess; ++j)
+            for (auto& g : b->groups)
+                if (e == cudaSuccess) e = batch_launch_step(g, j, b->cap);
+        for (auto& g : b->groups)
+            if (e == cudaSuccess) e = batch_launch_finalize(g, b->cap);
+        for (auto& g : b->groups)
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(g.host, g.bs, g.mem.size() * sizeof(BatchState), cudaMemcpyDeviceToHost, b->cap);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
+        if (e == cudaSuccess) e = e2;
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LBF_EDEVICE, std::string("batch graph: ") + cudaGetErrorString(e));
+        }
+    }
+    b->dirty = false;
+    return LBF_OK;
+}
+
+long long estimate_bytes(const lbf_domain_desc* ds, const lbf_scalar_desc* sd) {
+    const int vs = ds->velocity_set, q = vs_q(vs), d = vs_d(vs);
+    const long long N = ds->n[0] * ds->n[1] * (d == 3 ? ds->n[2] : 1);
+    const long long Np = (N + 63) / 64 * 64;
+    const long long sb = (long long)st_bytes(ds->storage), rb = (long long)rt_bytes(ds->storage);
+    const int nf = 1 + d + (sd ? 1 : 0);
+    long long b = 2 * q * Np * sb;                       // populations A/B
+    b += 4 * N + N + 8 * N;                              // mask, node types, set-up scratch
+    b += 2 * nf * N * rb;                                // residual moments
+    b += N * (d + 2) * 8;                                // observed moments (FP64)
+    if (ds->storage == LBF_STORE_F64) b += 4 * N;        // work list of the compacted sweep
+    if (sd) b += 2 * q * Np * rb + 3 * N * 8;            // scalar populations, q_ads, C_prev, C_init
+    const long long plane = N / std::min({ds->n[0], ds->n[1], d == 3 ? ds->n[2] : ds->n[1]});
+    b += 6 * 2 * 2 * (d + 1) * plane * rb;               // face layers (upper bound)
+    if (sd) b += 6 * 2 * q * plane * rb;                 // outflow snapshots (upper bound)
+    b += NSLOT * NACC * 8 + 4096;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+lbf_status lbf_domain_estimate_bytes(const lbf_domain_desc* desc, const lbf_scalar_desc* scalar, int64_t* bytes) {
+    if (!desc || !bytes) return fail(LBF_EINVAL, "null argument");
+    if (vs_q(desc->velocity_set) == 0) return fail(LBF_EUNSUPPORTED, "velocity set not built on the device");
+    for (int a = 0; a < 3; ++a)
+        if (desc->n[a] < 1 && (a < vs_d(desc->velocity_set))) return fail(LBF_EINVAL, "lattice dimensions must be >= 1");
+    *bytes = estimate_bytes(desc, scalar);
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_create(int64_t budget_bytes, int64_t residual_interval, lbf_batch** out) {
+    if (!out) return fail(LBF_EINVAL, "null argument");
+    *out = nullptr;
+    if (residual_interval < 1 || residual_interval > 100000) return fail(LBF_EINVAL, "residual_interval must be in [1, 1e5]");
+    if (budget_bytes < 0) return fail(LBF_EINVAL, "budget_bytes must be >= 0");
+    lbf_batch* b = new lbf_batch();
+    b->k = (int)residual_interval;
+    b->dev = current_device();
+    if (budget_bytes == 0) {
+        size_t fr = 0, tot = 0;
+        cudaError_t e = cudaMemGetInfo(&fr, &tot);
+        if (e != cudaSuccess) { delete b; return fail(LBF_EDEVICE, std::string("cudaMemGetInfo: ") + cudaGetErrorString(e)); }
+        budget_bytes = (int64_t)(0.9 * (double)fr);
+    }
+    b->budget = budget_bytes;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) { delete b; return fail(LBF_EDEVICE, std::string("batch: ") + cudaGetErrorString(e)); }
+    *out = b;
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_admit(lbf_batch* b, lbf_domain* D, int64_t max_iterations, double tol_density,
+                           double tol_velocity, double tol_scalar) {
+    if (!b || !D) return fail(LBF_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (D->batch) return fail(LBF_ESTATE, "the domain is already in a batch");
+    if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before lbf_batch_admit");
+    if (D->scalar) return fail(LBF_EUNSUPPORTED, "domains with a scalar are not batched");
+    if (max_iterations < 0) return fail(LBF_EINVAL, "max_iterations must be >= 0");
+    lbf_status st;
+    if ((st = ensure_mom(D))) return st;
+    if (b->bytes + D->bytes > b->budget)
+        return fail(LBF_ENOMEM, "batch memory budget exceeded (" + std::to_string(b->bytes + D->bytes) + " > " +
+                                    std::to_string(b->budget) + " bytes)");
+    if (D->last_stream) CK(cudaStreamSynchronize(D->last_stream));
+    b->members.push_back({D, max_iterations, {tol_density, tol_velocity, tol_scalar}});
+    D->batch = b;
+    b->bytes += D->bytes;
+    b->admitted.emplace_back(D, D->bytes);
+    b->dirty = true;
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_step(lbf_batch* b, int64_t nchunks, void* stream) {
+    if (!b) return fail(LBF_EINVAL, "null batch");
+    if (nchunks < 0) return fail(LBF_EINVAL, "nchunks < 0");
+    std::lock_guard<std::mutex> lock(b->mu);
+    cudaStream_t s = (cudaStream_t)stream;
+    lbf_status st;
+    if (b->dirty && (st = batch_rebuild(b, s))) return st;
+    if (b->members.empty() || nchunks == 0) return LBF_OK;
+    for (int64_t c = 0; c < nchunks; ++c) CK(cudaGraphLaunch(b->exec, s));
+    CK(cudaEventRecord(b->ev, s));
+    b->last = s;
+    b->launched = true;
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_poll(lbf_batch* b, lbf_domain** done, int32_t* status, int32_t cap, int32_t* ndone,
+                          int32_t wait) {
+    if (!b || !ndone || (cap > 0 && !done)) return fail(LBF_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lock(b->mu);
+    *ndone = 0;
+    if (b->launched) {
+        if (wait) {
+            CK(cudaEventSynchronize(b->ev));
+        } else {
+            const cudaError_t q = cudaEventQuery(b->ev);
+            if (q == cudaErrorNotReady) return LBF_OK;
+            if (q != cudaSuccess) return fail(LBF_EDEVICE, std::string("batch: ") + cudaGetErrorString(q));
+        }
+        batch_harvest(b);
+    }
+    int32_t n = 0;
+    while (n < cap && !b->finished.empty()) {
+        auto [D, code] = b->finished.front();
+        b->finished.erase(b->finished.begin());
+        batch_release(b, D);
+        done[n] = D;
+        if (status) status[n] = code;
+        ++n;
+    }
+    *ndone = n;
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_evict(lbf_batch* b, lbf_domain* D) {
+    if (!b || !D) return fail(LBF_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (D->batch != b) return fail(LBF_EINVAL, "the domain is not in this batch");
+    if (b->launched) CK(cudaEventSynchronize(b->ev));
+    if (b->launched) batch_harvest(b);
+    for (size_t i = 0; i < b->finished.size(); ++i)
+        if (b->finished[i].first == D) { b->finished.erase(b->finished.begin() + i); break; }
+    for (size_t i = 0; i < b->members.size(); ++i)
+        if (b->members[i].D == D) {
+            b->members.erase(b->members.begin() + i);
+            for (auto& g : b->groups)
+                for (auto& m : g.mem) m = m == (int)i ? -1 : (m > (int)i ? m - 1 : m);
+            b->dirty = true;
+            break;
+        }
+    batch_release(b, D);
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_info(lbf_batch* b, int64_t* running, int64_t* finished, int64_t* bytes, int64_t* budget) {
+    if (!b) return fail(LBF_EINVAL, "null batch");
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (running) *running = (int64_t)b->members.size();
+    if (finished) *finished = (int64_t)b->finished.size();
+    if (bytes) *bytes = b->bytes;
+    if (budget) *budget = b->budget;
+    return LBF_OK;
+}
+
+lbf_status lbf_batch_destroy(lbf_batch* b) {
+    if (!b) return LBF_OK;
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        if (b->launched) cudaEventSynchronize(b->ev);
+        for (auto& m : b->members) m.D->batch = nullptr;
+        for (auto& f : b->finished) f.first->batch = nullptr;
+    }
+    delete b;
+    return LBF_OK;
 }
 
 }  // extern "C"

@@ -121,9 +121,14 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
                 constexpr int i = Ii;
                 ((R*)P.gsrcp[i])[cell] = R(feq_i<L, double>(i, c0, u, uu));
             });
-            if (P.qads) ((R*)P.qads)[cell] = (mk & M_BB) ? R(I0.q0) : R(0);
-            if (P.cprev) ((R*)P.cprev)[cell] = R(c0);
         }
+    }
+    if constexpr (SCALAR) {
+        // every node, solid ones included: device memory comes uninitialised from the pool
+        if (P.qads) ((R*)P.qads)[cell] = (fluid && (mk & M_BB)) ? R(I0.q0) : R(0);
+        if (P.cprev) ((R*)P.cprev)[cell] = R(c0);
+    }
+    if (fluid) {
         if (P.mom_prev) {
             R* mp = (R*)P.mom_prev;
             mp[cell] = R(rho);

@@ -1,0 +1,193 @@
+"""A serving loop over `Batch`: solve requests arrive, are admitted while the
+device-memory budget allows, advance together, and leave with their fields.
+
+Requests (the serving mix): Poisson arrivals at rate `rate` per second; half
+(`cavity_frac`) are D2Q9 BGK lid-driven cavities with side log-uniform in
+[64, 1024], the others D3Q19 TRT porous channels with side log-uniform in
+[32, 160] and porosity uniform in [0.5, 0.9]; storage FP32 or FP16 deviation
+(half each); every request stops after `max_steps` steps or when its velocity
+residual drops below `tol_velocity` (checked every `residual_interval` steps,
+with the rule of `Domain.run`).  Everything is generated from one seed.
+
+`serve_batched` runs the requests through one `Batch`; `serve_sequential` runs
+them one at a time with `Domain.run` in arrival order (the same stop rule, so the
+same fields and step counts).  Both record per request the arrival, start and
+finish times (finish = after the density and velocity fields reached the host).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import cases
+from .batch import Batch, BatchFull, estimate_bytes
+from .core import Storage
+from .domain import Domain
+
+
+@dataclass
+class Request:
+    rid: int
+    kind: str            # "cavity" (D2Q9) or "channel" (D3Q19)
+    side: int
+    porosity: float
+    storage: Storage
+    arrival: float       # seconds after the start of the run
+    seed: int
+    params: object = None
+    est_bytes: int = 0
+
+
+@dataclass
+class Record:
+    rid: int
+    kind: str
+    nodes: int
+    arrival: float
+    start: float
+    finish: float
+    steps: int
+    status: int
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+def make_requests(n: int = 4000, rate: float = 50.0, seed: int = 1234, cavity_frac: float = 0.5,
+                  fp16_frac: float = 0.5, cavity_sides=(64, 1024), channel_sides=(32, 160),
+                  porosity=(0.5, 0.9)) -> List[Request]:
+    """The seeded serving mix; rate = inf puts every arrival at t = 0."""
+    rng = np.random.default_rng(seed)
+    gaps = np.zeros(n) if math.isinf(rate) else rng.exponential(1.0 / rate, n)
+    arrivals = np.cumsum(gaps) - (gaps[0] if n else 0.0)
+    reqs = []
+    for i in range(n):
+        cav = rng.random() < cavity_frac
+        lo, hi = cavity_sides if cav else channel_sides
+        side = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        por = float(rng.uniform(*porosity))
+        st = Storage.F16DEV if rng.random() < fp16_frac else Storage.F32
+        reqs.append(Request(i, "cavity" if cav else "channel", side, por, st, float(arrivals[i]),
+                            int(rng.integers(0, 2**31 - 1))))
+    return reqs
+
+
+def build_params(r: Request):
+    """momentum.Parameters of a request (geometry generated from its seed)."""
+    if r.kind == "cavity":
+        return cases.cavity_d2q9(r.side, 0.6, 0.1, r.storage)
+    n = [r.side] * 3
+    mask = cases.sphere_pack(n, r.porosity, 2.0, max(2.5, r.side / 16), r.seed, overlap=True)
+    return cases.porous_channel_d3q19(n, mask=mask, force=1e-5, storage=r.storage)
+
+
+def prepare(reqs: List[Request]) -> None:
+    """Build every request's parameters and device-byte estimate (client side, untimed)."""
+    for r in reqs:
+        r.params = build_params(r)
+        r.est_bytes = estimate_bytes(r.params)
+
+
+def _now(t0):
+    return time.perf_counter() - t0
+
+
+def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
+                  residual_interval: int = 50, budget_bytes: int = 0, chunks_per_poll: int = 1,
+                  create_ms: float = 20.0) -> List[Record]:
+    """Run the requests through one Batch; returns one Record per request.
+
+    The batch runs on its own CUDA stream.  While a chunk runs, the host builds
+    and initialises the domains of arrived requests on a second stream (for at
+    most `create_ms` per chunk); they join the batch at the next chunk.
+    Admission is by device-memory budget: a request waits until its byte
+    estimate fits.
+    """
+    import torch
+    max_it = max_steps - 2     # the rule stops after step t > max_iterations: max_steps steps in all
+    pending = sorted(reqs, key=lambda r: r.arrival)
+    records: List[Record] = []
+    live = {}
+    ready = []                 # (request, initialised domain) waiting for admission
+    s_batch, s_init = torch.cuda.Stream(), torch.cuda.Stream()
+    with Batch(budget_bytes, residual_interval) as batch:
+        budget = batch.info()["budget"]
+        used = 0
+        t0 = time.perf_counter()
+        i = 0
+
+        def create(limit_s):
+            nonlocal i, used
+            t_end = time.perf_counter() + limit_s
+            while i < len(pending) and pending[i].arrival <= _now(t0) and used + pending[i].est_bytes <= budget:
+                r = pending[i]
+                dom = Domain(r.params)
+                dom.init(s_init)
+                ready.append((r, dom))
+                used += r.est_bytes
+                i += 1
+                if time.perf_counter() > t_end:
+                    break
+            s_init.synchronize()
+
+        while i < len(pending) or live or ready:
+            if not live and not ready:
+                create(create_ms / 1e3)
+                if not ready:
+                    if i < len(pending):
+                        time.sleep(max(0.0, min(pending[i].arrival - _now(t0), 0.01)))
+                    continue
+            for r, dom in ready:
+                batch.admit(dom, max_it, tol_density=math.inf, tol_velocity=tol_velocity, tol_scalar=math.inf)
+                live[dom.h.value] = (r, dom, _now(t0))
+            ready.clear()
+            batch.step(chunks_per_poll, s_batch)
+            create(create_ms / 1e3)          # overlaps the chunk on the GPU
+            for dom, status in batch.poll(wait=True):
+                r, _, start = live.pop(dom.h.value)
+                dom.moments(s_batch)             # the fields reach the host
+                records.append(Record(r.rid, r.kind, int(np.prod(r.params.n[: r.params.dim])), r.arrival, start,
+                                      _now(t0), dom.time_step, status))
+                used -= r.est_bytes
+                dom.close()
+    return records
+
+
+def serve_sequential(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
+                     residual_interval: int = 50, stream=None) -> List[Record]:
+    """One solve at a time in arrival order with Domain.run (same stop rule)."""
+    max_it = max_steps - 2
+    records = []
+    t0 = time.perf_counter()
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        wait = r.arrival - _now(t0)
+        if wait > 0:
+            time.sleep(wait)
+        start = _now(t0)
+        with Domain(r.params) as dom:
+            dom.init(stream)
+            steps = dom.run(max_it, residual_interval, tol_density=math.inf, tol_velocity=tol_velocity,
+                            tol_scalar=math.inf, stream=stream)
+            dom.moments(stream)
+            conv = steps <= max_it + 1
+            records.append(Record(r.rid, r.kind, int(np.prod(r.params.n[: r.params.dim])), r.arrival, start,
+                                  _now(t0), steps, 1 if conv else 2))
+    return records
+
+
+def summary(records: List[Record]) -> dict:
+    if not records:
+        return {"solves": 0}
+    lat = np.array([r.latency for r in records])
+    t_first = min(r.arrival for r in records)
+    t_last = max(r.finish for r in records)
+    lups = sum(r.nodes * r.steps for r in records)
+    return {"solves": len(records), "seconds": t_last - t_first, "solves_per_s": len(records) / (t_last - t_first),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "mlups_all_nodes": lups / (t_last - t_first) / 1e6,
+            "converged": int(sum(r.status == 1 for r in records))}
