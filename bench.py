@@ -53,8 +53,9 @@ def parse():
                     help="pipelined bulk-copy sweep, one-shot staged sweep, or plain loads")
     ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
     ap.add_argument("--compact", type=int, default=-1, help="1/0: force the fluid work-list sweep on/off")
-    ap.add_argument("--workload", default="step", choices=["step", "serve"],
-                    help="step: the fused step on one lattice (headline); serve: the serving mix")
+    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch"],
+                    help="step: the fused step on one lattice (headline); serve: the serving mix; "
+                         "batch: batched vs single-domain sweeps and per-request host costs")
     ap.add_argument("--requests", type=int, default=300, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=float("inf"), help="serve: Poisson arrivals per second (inf = all at t=0)")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
@@ -342,6 +343,83 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_probe(args, rank, world, local_rank):
+    """Batched sweep vs single-domain sweep on one large domain and on many small
+    ones, and the host cost of one request's lifecycle (create, init, moments, destroy)."""
+    import math
+    import torch
+    from lbflow_b200 import cases, serve
+    from lbflow_b200.batch import Batch
+    from lbflow_b200.core import Storage
+    from lbflow_b200.domain import Domain
+    torch.cuda.set_device(local_rank)
+    sync = torch.cuda.synchronize
+    out = {"workload": "batch probe", "n_gpus": 1}
+    n = 192
+    mask = cases.sphere_pack([n] * 3, 0.7, 4.0, 10.0, args.seed)
+    nf = int(np.count_nonzero(mask == 0))
+    for st in (Storage.F32, Storage.F16DEV):
+        p = cases.porous_channel_d3q19([n] * 3, mask=mask, force=1e-6, storage=st)
+        with Domain(p) as d:
+            d.init().step(10)
+            sync()
+            t = time.perf_counter()
+            d.step(200)
+            sync()
+            out[f"single_{st.name}_mflups_{n}"] = nf * 200 / (time.perf_counter() - t) / 1e6
+        with Batch(0, 50) as b:
+            d = Domain(p).init()
+            b.admit(d, 10**6, math.inf, 0.0, math.inf)
+            b.step(1)
+            b.poll(wait=True)
+            sync()
+            t = time.perf_counter()
+            b.step(4)
+            b.poll(wait=True)
+            sync()
+            out[f"batched_{st.name}_mflups_{n}"] = nf * 200 / (time.perf_counter() - t) / 1e6
+            b.evict(d)
+            d.close()
+    doms = [Domain(cases.cavity_d2q9(64, 0.6, 0.1, Storage.F32)).init() for _ in range(64)]
+    for d in doms:
+        d.step(1)
+    sync()
+    t = time.perf_counter()
+    for d in doms:
+        d.step(100)
+    sync()
+    out["small_64x64sq_single_domain_steps_per_s"] = 64 * 100 / (time.perf_counter() - t)
+    with Batch(0, 50) as b:
+        for d in doms:
+            b.admit(d, 10**6, math.inf, 0.0, math.inf)
+        b.step(1)
+        b.poll(wait=True)
+        sync()
+        t = time.perf_counter()
+        b.step(2)
+        b.poll(wait=True)
+        sync()
+        out["small_64x64sq_batched_domain_steps_per_s"] = 64 * 100 / (time.perf_counter() - t)
+        for d in doms:
+            b.evict(d)
+    for d in doms:
+        d.close()
+    reqs = serve.make_requests(40, float("inf"), 77)
+    serve.prepare(reqs)
+    tc = ti = tm = tx = 0.0
+    for r in reqs:
+        t = time.perf_counter(); d = Domain(r.params); tc += time.perf_counter() - t
+        t = time.perf_counter(); d.init(); sync(); ti += time.perf_counter() - t
+        d.step(10)
+        sync()
+        t = time.perf_counter(); d.moments(); tm += time.perf_counter() - t
+        t = time.perf_counter(); d.close(); tx += time.perf_counter() - t
+    out["request_ms"] = {"create": 1e3 * tc / 40, "init": 1e3 * ti / 40, "moments": 1e3 * tm / 40,
+                         "destroy": 1e3 * tx / 40}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -356,6 +434,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "serve":
         run_serve(args, rank, world, local_rank)
+    elif args.workload == "batch":
+        run_batch_probe(args, rank, world, local_rank)
     else:
         run_engine(args, rank, world, local_rank)
         if world > 1:
