@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
     ap.add_argument("--chunk", type=int, default=50, help="serve: residual interval (steps per chunk)")
     ap.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time baseline")
+    ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
+                    help="N > 1: z-slabs of one n x n x (n N) channel with a halo exchange per step, "
+                         "or independent replicas")
     return ap.parse_args()
 
 
@@ -343,6 +346,78 @@ def run_serve(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_slabs(args, rank, world, local_rank):
+    """Weak scaling over z-slabs: rank r owns an n^3 slab of an n x n x (n * world)
+    channel (no-slip y and z walls at the ends, periodic x), exchanges its halo
+    planes with its neighbours after every step (NCCL send/recv)."""
+    import torch
+    import torch.distributed as dist
+    from lbflow_b200 import slab
+    torch.cuda.set_device(local_rank)
+    dist.barrier()        # the first collective of the group includes every rank
+    own = geometry(args.n, args.seed + rank, args.porosity).reshape(args.n, args.n, args.n)
+    p = params_for(args, own.ravel())
+    p.n = [args.n, args.n, args.n * world]
+    ex = slab.TorchExchange(rank, world, periodic=False)
+    stream = torch.cuda.current_stream()
+    t_e2e0 = time.perf_counter()
+    sd = slab.SlabDomain(p, rank, world, ex, own_mask=own)
+    sd.init()
+    n_fluid = sd.n_fluid_own
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        sd.step(args.warmup)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        start.record(stream)
+        sd.step(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    rho, u = sd.moments()                      # the fields reach the host
+    e2e_sec = time.perf_counter() - t_e2e0
+    t = torch.tensor([ms, e2e_sec, float(n_fluid)], device="cuda", dtype=torch.float64)
+    tmax = t.clone()
+    dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    tsum = t.clone()
+    dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+    dist.barrier()
+    sd.close()
+    if rank != 0:
+        return
+    ms, e2e_sec, fluid_all = float(tmax[0]), float(tmax[1]), float(tsum[2])
+    sec = ms / 1e3
+    mlups = fluid_all * args.steps / sec / 1e6
+    s_b = SBYTES[args.storage]
+    alg_bytes = n_fluid * 2 * 19 * s_b + args.n ** 3
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (sec / args.steps) / 1e9
+    halo = 2 * 5 * args.n * args.n * s_b
+    line = {"metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64",
+            "data": "synthetic (seeded sphere packing per slab)",
+            "config": {"workload": f"D3Q19 TRT porous channel {args.n}x{args.n}x{args.n * world} in z-slabs of "
+                                   f"{args.n}^3 per GPU (tau+=0.8, magic 1/4, g_x=1e-6, spheres r in [4,10], "
+                                   f"porosity {args.porosity:g}, periodic x, no-slip y/z)",
+                       "storage": args.storage, "n_fluid": int(fluid_all), "parallelism": f"z-slabs x{world}",
+                       "halo_bytes_per_step_per_gpu": 2 * halo,
+                       "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N per GPU)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profile_traffic(args.storage, args.n), "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "note": "per GPU, step kernel + halo exchange in the timed step"},
+            "cpu_baseline": None,
+            "e2e": {"value": fluid_all * args.steps / e2e_sec / 1e6, "unit": "MLUPS",
+                    "h2d_bytes_per_step": args.n ** 3 * world / args.steps,
+                    "d2h_bytes_per_step": args.n ** 3 * 4 * 8 * world / args.steps,
+                    "note": "SlabDomain: node-type upload, init, warm-up + K steps with halos, moments download"},
+            "gpu_launches": args.steps * (3 + sum(x is not None for x in slab.neighbours(0, world, False))),
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_batch_probe(args, rank, world, local_rank):
     """Batched sweep vs single-domain sweep on one large domain and on many small
     ones, and the host cost of one request's lifecycle (create, init, moments, destroy)."""
@@ -436,6 +511,8 @@ def main():
         run_serve(args, rank, world, local_rank)
     elif args.workload == "batch":
         run_batch_probe(args, rank, world, local_rank)
+    elif world > 1 and args.decomp == "slab":
+        run_slabs(args, rank, world, local_rank)
     else:
         run_engine(args, rank, world, local_rank)
         if world > 1:

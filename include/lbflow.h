@@ -219,8 +219,13 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  *                  nodes sharing a 32-byte sector with them) instead of the dense
  *                  lattice; default on for FP64 storage only (where it is faster); set
  *                  before lbf_domain_init.  get: 1 when in effect.
+ * LBF_OPT_Z_BEGIN, LBF_OPT_Z_END  planes [z_begin, z_end) that steps, observation and
+ *                  inventories cover (default all); set before lbf_domain_init.  A
+ *                  z-slab of a larger lattice sweeps its owned planes and keeps one
+ *                  ghost plane on each side (see the halo calls below).
  * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
-enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4 };
+enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4,
+       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */
@@ -228,6 +233,26 @@ lbf_status lbf_domain_time_step(lbf_domain* dom, int64_t* t);
 /* Device bytes held by the domain. */
 lbf_status lbf_domain_device_bytes(lbf_domain* dom, int64_t* bytes);
 lbf_status lbf_domain_destroy(lbf_domain* dom);
+
+/* ---- z-slab halos (multi-GPU decomposition) ------------------------------ */
+/* No counterpart in the reference (one process, one lattice).  A lattice split
+ * into z-slabs across GPUs runs one domain per slab: its owned planes
+ * [z_begin, z_end) plus one ghost plane below and above (LBF_OPT_Z_*), with
+ * periodic z faces locally.  A ghost plane is either the neighbour's boundary
+ * plane (filled by the halo exchange after every step) or solid nodes (a no-slip
+ * wall of the whole lattice, folded into the link bits like any solid).  After
+ * each step, lbf_domain_halo_pack(face) gathers the populations that leave the
+ * owned boundary plane through `face` (LBF_BOTTOM: c_z = -1, LBF_TOP: c_z = +1,
+ * ascending direction index) into a contiguous device buffer for the neighbour;
+ * lbf_domain_halo_unpack(face) scatters the neighbour's buffer into the ghost plane
+ * beyond `face` (the directions the next step pulls from it).  A bottom pack
+ * pairs with the lower neighbour's top unpack, and a top pack with the upper
+ * neighbour's bottom unpack.  lbf_domain_halo_info gives the number of leaving
+ * directions per face, the nodes per plane and the buffer bytes per face.
+ * Asynchronous on `stream`. */
+lbf_status lbf_domain_halo_info(lbf_domain* dom, int32_t* ndir, int64_t* plane_nodes, int64_t* bytes);
+lbf_status lbf_domain_halo_pack(lbf_domain* dom, int32_t face, void* dst, void* stream);
+lbf_status lbf_domain_halo_unpack(lbf_domain* dom, int32_t face, const void* src, void* stream);
 
 /* ---- FP64 fluid sums with no device allocation --------------------------- */
 /* No counterpart in the reference (whose reductions are rayon sums on the CPU).

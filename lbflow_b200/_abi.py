@@ -24,7 +24,7 @@ LBF_INNER_ANTI_BOUNCE_BACK, LBF_INNER_BOUNCE_BACK = range(2)
 LBF_STORE_F64, LBF_STORE_F32, LBF_STORE_F16DEV, LBF_STORE_BF16DEV = range(4)
 LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 
-LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT = range(5)
+LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END = range(7)
 
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2
@@ -106,6 +106,9 @@ SIGNATURES = {
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),
     "lbf_inventory_noalloc": (_I32, [_P, _P, _P, _P, _P, _I64, _I32, _P, _P]),
+    "lbf_domain_halo_info": (_I32, [_P, _PI32, _PI64, _PI64]),
+    "lbf_domain_halo_pack": (_I32, [_P, _I32, _P, _P]),
+    "lbf_domain_halo_unpack": (_I32, [_P, _I32, _P, _P]),
     "lbf_domain_estimate_bytes": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _PI64]),
     "lbf_batch_create": (_I32, [_I64, _I64, C.POINTER(_P)]),
     "lbf_batch_admit": (_I32, [_P, _P, _I64, _D, _D, _D]),

@@ -251,6 +251,7 @@ struct lbf_domain {
     int pipe_stages = 0;          // 0 = chosen from the shared-memory budget
     bool compact = false;         // compacted sweep over a work list on the lean path (in effect)
     int compact_opt = -1;         // -1 = default (FP64 storage only), 0 off, 1 on
+    long long z_begin = 0, z_end = 0;   // planes swept (0, 0 = all); a z-slab sweeps its owned planes
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
     long long nlist = 0;
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
@@ -297,8 +298,12 @@ dim3 step_block(const lbf_domain* D) {
     }
     return dim3(bx, 1, 1);
 }
+long long zb(const lbf_domain* D) { return D->z_end > 0 ? D->z_begin : 0; }
+long long ze(const lbf_domain* D) { return D->z_end > 0 ? D->z_end : D->n[2]; }
+bool z_restricted(const lbf_domain* D) { return zb(D) != 0 || ze(D) != D->n[2]; }
+
 dim3 step_grid(const lbf_domain* D, dim3 b) {
-    return dim3((unsigned)((D->n[0] + b.x - 1) / b.x), (unsigned)D->n[1], (unsigned)D->n[2]);
+    return dim3((unsigned)((D->n[0] + b.x - 1) / b.x), (unsigned)D->n[1], (unsigned)(ze(D) - zb(D)));
 }
 
 bool mom_kind_ok(const lbf_domain_desc& ds, int vs, int f, std::string& why) {
@@ -481,7 +486,7 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     }
     D->nlist = 0;
     if (D->list) { dev_free(D->list, D->dev); D->list = nullptr; }
-    const bool want = D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0;
+    const bool want = (D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0) && !z_restricted(D);
     D->compact = want;
     if (!D->facebc && !D->scalar && want && N < (1ll << 30) && (st = build_list(D, s))) return st;
     D->prepared = true;
@@ -498,6 +503,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.nlist = D->nlist;
     P.inv_nx = 1.0 / (double)D->n[0];
     P.inv_ny = 1.0 / (double)D->n[1];
+    P.z0 = (int)zb(D);
     const size_t eb = st_bytes(D->st);
     for (int i = 0; i < D->q; ++i) {
         P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->Np * eb;
@@ -559,6 +565,7 @@ bool can_stage(const lbf_domain* D) {
 
 // Whether the pipelined sweep applies (lean path, aligned rows, two stages fit).
 bool can_pipe(const lbf_domain* D) {
+    if (z_restricted(D)) return false;
     const size_t rowb = D->n[0] * st_bytes(D->st);
     return !D->facebc && !D->scalar && rowb % 16 == 0 && 2 * D->q * rowb <= 200 * 1024;
 }
@@ -644,6 +651,7 @@ lbf_status ensure_mom(lbf_domain* D) {
 
 lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     lbf_status st;
+    if (D->z_end > 0 && D->z_begin >= D->z_end) return fail(LBF_EINVAL, "swept z planes: need z_begin < z_end");
     if (!D->prepared && (st = prepare(D, nullptr, nullptr, s))) return st;
     if ((st = ensure_mom(D))) return st;
     StepParams P;
@@ -722,6 +730,55 @@ lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
     P.obs_c = D->obs + D->N * (1 + D->d);
     cudaError_t e = launch_step_any(D, P, s);
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("observe kernel: ") + cudaGetErrorString(e));
+    return LBF_OK;
+}
+
+void tables_c(int vs, int i, int* c) {
+    for (int a = 0; a < 3; ++a)
+        c[a] = vs == LBF_D2Q9 ? (a < 2 ? Lat<VS_D2Q9>::c(i, a) : 0)
+             : vs == LBF_D3Q19 ? Lat<VS_D3Q19>::c(i, a) : Lat<VS_D3Q27>::c(i, a);
+}
+
+// Pack (unpack = false) the leaving directions of the owned boundary plane of
+// `face` into buf, or unpack (true) buf into the entering directions of the
+// ghost plane beyond it, in the state the next step reads (buffer t & 1).
+lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream_t s) {
+    if (!D || !buf) return fail(LBF_EINVAL, "null argument");
+    if (D->d != 3) return fail(LBF_EINVAL, "halos apply to 3-D lattices");
+    if (face != LBF_BOTTOM && face != LBF_TOP) return fail(LBF_EINVAL, "halo face must be LBF_BOTTOM or LBF_TOP");
+    if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
+    const long long z0 = zb(D), z1 = ze(D);
+    if (z0 < 1 || z1 > D->n[2] - 1) return fail(LBF_EINVAL, "halos need a ghost plane below z_begin and above z_end - 1");
+    // bottom: pack plane z0, c_z = -1; unpack ghost z0 - 1, c_z = +1
+    // top:    pack plane z1 - 1, c_z = +1; unpack ghost z1, c_z = -1
+    const bool bottom = face == LBF_BOTTOM;
+    const int want = bottom ? (unpack ? +1 : -1) : (unpack ? -1 : +1);
+    const long long z = bottom ? (unpack ? z0 - 1 : z0) : (unpack ? z1 : z1 - 1);
+    const long long plane = D->n[0] * D->n[1];
+    const size_t eb = st_bytes(D->st);
+    HaloPlanes H{};
+    H.plane = plane;
+    for (int i = 0; i < D->q; ++i) {
+        int c[3];
+        tables_c(D->vs, i, c);
+        if (c[2] != want) continue;
+        H.planes[H.nd++] = (char*)D->pop[D->t & 1] + ((size_t)i * D->Np + (size_t)(z * plane)) * eb;
+    }
+    const long long n = (long long)H.nd * plane;
+    const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 4 * 148);
+    if (eb == 8) {
+        if (unpack) k_halo_unpack<double><<<blocks, 256, 0, s>>>(H, (const double*)buf);
+        else k_halo_pack<double><<<blocks, 256, 0, s>>>(H, (double*)buf);
+    } else if (eb == 4) {
+        if (unpack) k_halo_unpack<float><<<blocks, 256, 0, s>>>(H, (const float*)buf);
+        else k_halo_pack<float><<<blocks, 256, 0, s>>>(H, (float*)buf);
+    } else {
+        if (unpack) k_halo_unpack<unsigned short><<<blocks, 256, 0, s>>>(H, (const unsigned short*)buf);
+        else k_halo_pack<unsigned short><<<blocks, 256, 0, s>>>(H, (unsigned short*)buf);
+    }
+    CK(cudaGetLastError());
+    D->last_stream = s;
     return LBF_OK;
 }
 
@@ -835,6 +892,7 @@ lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
     if (!D || !s) return fail(LBF_EINVAL, "null argument");
     if (D->scalar) return fail(LBF_EINVAL, "one scalar per domain");
     if (D->initialized || D->prepared) return fail(LBF_ESTATE, "attach the scalar before lbf_domain_init");
+    if (z_restricted(D)) return fail(LBF_EUNSUPPORTED, "z-slab domains with a scalar are not built");
     if (s->velocity_set != D->vs)
         return fail(LBF_EUNSUPPORTED, "on the device the scalar uses the momentum velocity set");
     if (D->st != LBF_STORE_F64 && D->st != LBF_STORE_F32)
@@ -973,13 +1031,18 @@ lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     if ((st = do_observe(D, s))) return st;
     const long long N = D->N;
     const double* c = D->scalar ? D->obs + N * (1 + D->d) : nullptr;
-    const unsigned nb = (unsigned)((N + 255) / 256);
+    // the swept planes only (all of them unless the domain is a z-slab)
+    const long long o = zb(D) * D->n[0] * D->n[1], M = (ze(D) - zb(D)) * D->n[0] * D->n[1];
+    const unsigned nb = (unsigned)((M + 255) / 256);
+    const double* rho = D->obs + o;
+    const double* uu = D->obs + N + o * D->d;
+    const double* cc = c ? c + o : nullptr;
     if (D->d == 2) {
-        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask, N, D->obs, D->obs + N, c, (const double*)D->qads, D->accum);
-        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask, N, D->obs, D->obs + N, c, (const float*)D->qads, D->accum);
+        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum);
+        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum);
     } else {
-        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask, N, D->obs, D->obs + N, c, (const double*)D->qads, D->accum);
-        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask, N, D->obs, D->obs + N, c, (const float*)D->qads, D->accum);
+        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum);
+        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum);
     }
     CK(cudaGetLastError());
     double* tmp = nullptr;
@@ -1032,6 +1095,14 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
             if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_COMPACT before lbf_domain_init");
             D->compact_opt = value != 0 ? 1 : 0;
             return LBF_OK;
+        case LBF_OPT_Z_BEGIN:
+        case LBF_OPT_Z_END:
+            if (D->prepared) return fail(LBF_ESTATE, "set the swept z planes before lbf_domain_init");
+            if (D->d != 3) return fail(LBF_EINVAL, "z planes apply to 3-D lattices");
+            if (D->scalar) return fail(LBF_EUNSUPPORTED, "z-slab domains with a scalar are not built");
+            if (value < 0 || value > D->n[2]) return fail(LBF_EINVAL, "z plane out of range");
+            (option == LBF_OPT_Z_BEGIN ? D->z_begin : D->z_end) = value;
+            return LBF_OK;
         default:
             return fail(LBF_EINVAL, "unknown option");
     }
@@ -1045,6 +1116,8 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
         case LBF_OPT_PIPE: *value = (D->pipe && can_pipe(D)) ? 1 : 0; return LBF_OK;
         case LBF_OPT_PIPE_STAGES: *value = D->pipe_stages; return LBF_OK;
         case LBF_OPT_COMPACT: *value = (D->compact && D->list) ? 1 : 0; return LBF_OK;
+        case LBF_OPT_Z_BEGIN: *value = zb(D); return LBF_OK;
+        case LBF_OPT_Z_END: *value = ze(D); return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
     }
 }
@@ -1056,6 +1129,30 @@ lbf_status lbf_domain_destroy(lbf_domain* D) {
         delete D;
     }
     return LBF_OK;
+}
+
+lbf_status lbf_domain_halo_info(lbf_domain* D, int32_t* ndir, int64_t* plane_nodes, int64_t* bytes) {
+    if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->d != 3) return fail(LBF_EINVAL, "halos apply to 3-D lattices");
+    int nd = 0;
+    for (int i = 0; i < D->q; ++i) {
+        int c[3];
+        tables_c(D->vs, i, c);
+        nd += c[2] < 0;
+    }
+    const long long plane = D->n[0] * D->n[1];
+    if (ndir) *ndir = nd;
+    if (plane_nodes) *plane_nodes = plane;
+    if (bytes) *bytes = (int64_t)nd * plane * (int64_t)st_bytes(D->st);
+    return LBF_OK;
+}
+
+lbf_status lbf_domain_halo_pack(lbf_domain* D, int32_t face, void* dst, void* stream) {
+    return halo_copy(D, face, false, dst, (cudaStream_t)stream);
+}
+
+lbf_status lbf_domain_halo_unpack(lbf_domain* D, int32_t face, const void* src, void* stream) {
+    return halo_copy(D, face, true, const_cast<void*>(src), (cudaStream_t)stream);
 }
 
 lbf_status lbf_solve(const lbf_domain_desc* desc, const lbf_scalar_desc* sdesc, int64_t nsteps, double* rho,
@@ -1405,6 +1502,7 @@ lbf_status lbf_batch_admit(lbf_batch* b, lbf_domain* D, int64_t max_iterations, 
     if (D->batch) return fail(LBF_ESTATE, "the domain is already in a batch");
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before lbf_batch_admit");
     if (D->scalar) return fail(LBF_EUNSUPPORTED, "domains with a scalar are not batched");
+    if (z_restricted(D)) return fail(LBF_EUNSUPPORTED, "z-slab domains are not batched");
     if (max_iterations < 0) return fail(LBF_EINVAL, "max_iterations must be >= 0");
     lbf_status st;
     if ((st = ensure_mom(D))) return st;

@@ -90,6 +90,7 @@ struct StepParams {
     const uint32_t* list;     // compacted sweep: work entries (see k_step_list)
     long long nlist;
     double inv_nx, inv_ny;    // 1/nx, 1/ny for index -> coordinate conversion
+    int z0, zpad;             // first z plane of the dense sweep (slab domains sweep [z0, z0 + gridDim.z))
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -970,7 +971,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
     } else {
         g.x = blockIdx.x * blockDim.x + threadIdx.x;
         g.y = blockIdx.y;
-        g.z = blockIdx.z;
+        g.z = blockIdx.z + P.z0;
         inside = g.x < P.nx;
         if (!inside) g.x = 0;
     }
@@ -1311,6 +1312,35 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
         }
     }
     if (P.residual) block_accumulate<5>(racc, P.accum);
+}
+
+// =================================================================== z-slab halos
+// A z-slab domain holds its owned planes plus one ghost plane below and above.
+// After a step the owned boundary plane's populations that leave the slab (c_z
+// = -1 at the bottom, +1 at the top) are packed into a contiguous buffer for the
+// neighbour, and the neighbour's buffer is unpacked into the ghost plane, whose
+// entering directions (c_z = +1 below, -1 above) the next step pulls.
+// planes[k] = element pointer of direction dirs[k] at the plane's first node.
+struct HaloPlanes {
+    void* planes[9];
+    int nd;
+    long long plane;   // nodes per plane
+};
+template <class T>
+__global__ void k_halo_pack(HaloPlanes H, T* buf) {
+    const long long n = (long long)H.nd * H.plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i / H.plane);
+        buf[i] = ((const T*)H.planes[k])[i - k * H.plane];
+    }
+}
+template <class T>
+__global__ void k_halo_unpack(HaloPlanes H, const T* buf) {
+    const long long n = (long long)H.nd * H.plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i / H.plane);
+        ((T*)H.planes[k])[i - k * H.plane] = buf[i];
+    }
 }
 
 }  // namespace lbf
