@@ -49,13 +49,25 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block", type=int, default=0, help="override the x block size")
-    ap.add_argument("--sweep", default="plain", choices=["pipe", "stage", "plain"],
-                    help="pipelined bulk-copy sweep, one-shot staged sweep, or plain loads")
+    ap.add_argument("--sweep", default="auto", choices=["auto", "pipe", "stage", "plain", "sparse"],
+                    help="auto: the library's default (the fluid-only sparse layout for porous lean lattices); "
+                         "pipelined bulk-copy sweep, one-shot staged sweep, plain dense loads, or sparse")
     ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
     ap.add_argument("--compact", type=int, default=-1, help="1/0: force the fluid work-list sweep on/off")
-    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch"],
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the sweep variant and block size by timing candidates first (untimed)")
+    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy"],
                     help="step: the fused step on one lattice (headline); serve: the serving mix; "
-                         "batch: batched vs single-domain sweeps and per-request host costs")
+                         "batch: batched vs single-domain sweeps and per-request host costs; "
+                         "accuracy: FP32 / FP16 / BF16 storage against FP64 at full size (--case)")
+    ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],
+                    help="accuracy: c2 porous channel 256^3 (5000 steps), c3 D3Q27 MRT Taylor-Green 384^3 "
+                         "(10000 steps), c4 packed bed with scalar 192x192x384 (20000 steps)")
+    ap.add_argument("--acc-steps", type=int, default=0, help="accuracy: override the number of steps")
+    ap.add_argument("--c4-collision", default="trt0.55", choices=["bgk0.6", "bgk0.8", "trt0.8", "trt0.55"],
+                    help="accuracy c4: momentum collision (BGK tau 0.6 / 0.8, or TRT tau+ 0.8 / 0.55 magic 1/4)")
+    ap.add_argument("--c4-u", type=float, default=0.01, help="accuracy c4: inlet velocity u_z")
+    ap.add_argument("--c3-re", type=float, default=1600.0, help="accuracy c3: Reynolds number of the vortex")
     ap.add_argument("--requests", type=int, default=300, help="serve: number of requests")
     ap.add_argument("--rate", type=float, default=float("inf"), help="serve: Poisson arrivals per second (inf = all at t=0)")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
@@ -226,19 +238,31 @@ def run_engine(args, rank, world, local_rank):
     n_fluid = int(np.count_nonzero(mask == 0))
     N = mask.size
     stream = torch.cuda.current_stream()
+    tuned = None
+    if args.autotune:
+        from lbflow_b200 import autotune
+        tuned = autotune.autotune(p, steps=20, cache=None)
     dom = Domain(p)
+    if tuned is not None:
+        from lbflow_b200 import autotune
+        autotune.apply(dom, tuned)
     if args.block:
         dom.set_option(_abi.LBF_OPT_BLOCK_X, args.block)
-    dom.set_option(_abi.LBF_OPT_PIPE, 1 if args.sweep == "pipe" else 0)
-    dom.set_option(_abi.LBF_OPT_STAGE, 1 if args.sweep == "stage" else 0)
+    if tuned is None and args.sweep != "auto":
+        dom.set_option(_abi.LBF_OPT_PIPE, 1 if args.sweep == "pipe" else 0)
+        dom.set_option(_abi.LBF_OPT_STAGE, 1 if args.sweep == "stage" else 0)
+        dom.set_option(_abi.LBF_OPT_SPARSE, 1 if args.sweep == "sparse" else 0)
     if args.stages:
         dom.set_option(_abi.LBF_OPT_PIPE_STAGES, args.stages)
     if args.compact >= 0:
         dom.set_option(_abi.LBF_OPT_COMPACT, args.compact)
     dom.init(stream)
-    sweep = ("pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
+    sweep = ("sparse fluid-only layout" if dom.get_option(_abi.LBF_OPT_SPARSE) else
+             "pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
              "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else
              "compacted fluid work list" if dom.get_option(_abi.LBF_OPT_COMPACT) else "dense lattice")
+    if tuned is not None:
+        sweep += f" (autotuned: {tuned.get('sweep')}, block_x {tuned.get('block_x', 0)})"
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     # the clock sampler starts before the warm-up so that its samples cover the timed steps
     with Clocks(local_rank) as clk:
@@ -418,6 +442,116 @@ def run_slabs(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_accuracy(args, rank, world, local_rank):
+    """Full-size runs of one configuration in every storage format, each compared
+    with the FP64-storage run of the same engine (which matches the FP64 oracle to
+    1e-11 relative L2 on the parity cases): relative L2 over fluid nodes of velocity
+    and density at the final step, plus the case's physical observable (kinetic
+    energy for the vortex, outlet concentration and FP64 inventories for the bed)."""
+    import math
+    import torch
+    from lbflow_b200 import _abi, cases
+    from lbflow_b200.core import Storage
+    from lbflow_b200.domain import Domain
+    torch.cuda.set_device(local_rank)
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+    out = {"workload": f"accuracy {args.case}", "n_gpus": 1, "runs": {}}
+    if args.case == "c2":
+        steps = args.acc_steps or 5000
+        mask = geometry(256, args.seed, 0.7)
+        stores = [Storage.F64, Storage.F32, Storage.F16DEV, Storage.BF16DEV]
+        mk = lambda st: cases.porous_channel_d3q19([256] * 3, mask=mask, force=1e-6, storage=st)  # noqa: E731
+        sample = []
+    elif args.case == "c3":
+        steps = args.acc_steps or 10000
+        stores = [Storage.F64, Storage.F32, Storage.F16DEV]
+        mk = lambda st: cases.tgv_d3q27(384, 0.05, args.c3_re, st)[0]  # noqa: E731
+        out["c3_re"] = args.c3_re
+        sample = list(range(0, steps + 1, 500))
+    else:
+        steps = args.acc_steps or 40000
+        stores = [Storage.F64, Storage.F32]
+        n = [192, 192, 384]
+        # porosity 0.6 is below the jamming limit of non-overlapping random spheres,
+        # so spheres may overlap; 8 clear layers at the inlet and the outlet keep the
+        # Zou-He inlet from feeding closed pockets
+        mask = cases.sphere_pack(n, 0.6, 4.0, 10.0, args.seed, overlap=True).reshape(n[2], n[1], n[0])
+        mask[:8] = 0
+        mask[-8:] = 0
+        mask = mask.ravel()
+        from lbflow_b200.core import BGK, TRT
+        coll = {"bgk0.6": BGK(0.6), "bgk0.8": BGK(0.8), "trt0.8": TRT.from_magic(0.8, 0.25),
+                "trt0.55": TRT.from_magic(0.55, 0.25)}[args.c4_collision]
+        mk = lambda st: cases.packed_bed_scalar(n, mask=mask, storage=st, collision=coll, u_in=args.c4_u)  # noqa: E731
+        out["c4"] = {"collision": args.c4_collision, "u_in": args.c4_u, "buffer_layers": 8}
+        sample = list(range(0, steps + 1, 2000))
+    ref = None
+    for st in stores:
+        p = mk(st)
+        scal = None
+        if isinstance(p, tuple):
+            p, scal = p
+        curve = []
+        t_run = 0.0
+        with Domain(p, scal) as d:
+            d.init()
+            cls, _ = d.node_class()
+            fl = (cls & _abi.LBF_CLASS_SOLID) == 0
+            t = 0
+            for target in (sample if sample else [steps]):
+                if target > t:
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    d.step(target - t)
+                    torch.cuda.synchronize()
+                    t_run += time.perf_counter() - t0
+                    t = target
+                if sample:
+                    rho, u, c = d.moments()
+                    if args.case == "c3":
+                        curve.append(float(0.5 * np.sum(rho * np.sum(u * u, axis=1)) / rho.size))
+                    else:
+                        pl = n[0] * n[1]
+                        out_fl = fl[-pl:]
+                        inv = d.inventory()
+                        curve.append([float(np.mean(c[-pl:][out_fl])), *[float(x) for x in inv]])
+            rho, u, c = d.moments()
+        n_fluid = int(np.count_nonzero(fl))
+        run = {"mflups": n_fluid * steps / t_run / 1e6 if t_run > 0 else None, "steps": steps}
+        if ref is None:
+            ref = (rho[fl], u[fl], None if c is None else c[fl], curve)
+        else:
+            run["rel_l2_velocity"] = rel(u[fl], ref[1])
+            run["rel_l2_density"] = rel(rho[fl], ref[0])
+            run["rel_l2_density_deviation"] = rel(rho[fl] - 1.0, ref[0] - 1.0)
+            if c is not None:
+                run["rel_l2_scalar"] = rel(c[fl], ref[2])
+            if args.case == "c3":
+                e, e0 = np.array(curve), np.array(ref[3])
+                run["energy_max_rel_dev"] = float(np.max(np.abs(e - e0) / e0))
+            elif args.case == "c4":
+                a, b = np.array(curve), np.array(ref[3])
+                run["outlet_c_max_abs_dev"] = float(np.max(np.abs(a[:, 0] - b[:, 0])))
+                run["inventory_max_rel_dev"] = [float(np.max(np.abs(a[:, k] - b[:, k]) /
+                                                             np.maximum(np.abs(b[:, k]), 1e-300)))
+                                                for k in range(1, a.shape[1])]
+        if curve:
+            run["curve_steps"] = sample
+            run["curve"] = curve
+        out["runs"][st.name] = run
+    if args.case == "c3":
+        nu = 0.05 * (384 / (2 * math.pi)) / args.c3_re
+        k2 = 3 * (2 * math.pi / 384) ** 2
+        e = np.array(out["runs"]["F64"]["curve"])
+        out["c3_early_decay_vs_exp(-2 nu k^2 t)"] = float(abs(e[1] / e[0] - math.exp(-2 * nu * k2 * 500)) /
+                                                          (1 - math.exp(-2 * nu * k2 * 500)))
+    print(json.dumps(out), flush=True)
+
+
 def run_batch_probe(args, rank, world, local_rank):
     """Batched sweep vs single-domain sweep on one large domain and on many small
     ones, and the host cost of one request's lifecycle (create, init, moments, destroy)."""
@@ -511,6 +645,8 @@ def main():
         run_serve(args, rank, world, local_rank)
     elif args.workload == "batch":
         run_batch_probe(args, rank, world, local_rank)
+    elif args.workload == "accuracy":
+        run_accuracy(args, rank, world, local_rank)
     elif world > 1 and args.decomp == "slab":
         run_slabs(args, rank, world, local_rank)
     else:

@@ -223,9 +223,14 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  *                  inventories cover (default all); set before lbf_domain_init.  A
  *                  z-slab of a larger lattice sweeps its owned planes and keeps one
  *                  ghost plane on each side (see the halo calls below).
+ * LBF_OPT_SPARSE   1 = on the lean path, store the populations of the fluid nodes only
+ *                  and sweep them (no solid bytes move, every thread updates a fluid
+ *                  node); 0 = dense layout; default: sparse on the lean path when at
+ *                  least 5 % of the nodes are solid.  Set before lbf_domain_init.
+ *                  get: 1 when in effect.
  * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
 enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4,
-       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6 };
+       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6, LBF_OPT_SPARSE = 7 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */

@@ -24,7 +24,8 @@ LBF_INNER_ANTI_BOUNCE_BACK, LBF_INNER_BOUNCE_BACK = range(2)
 LBF_STORE_F64, LBF_STORE_F32, LBF_STORE_F16DEV, LBF_STORE_BF16DEV = range(4)
 LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 
-LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END = range(7)
+(LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END,
+ LBF_OPT_SPARSE) = range(8)
 
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2

@@ -137,7 +137,7 @@ def packed_bed_scalar(n: Sequence[int] = (192, 192, 384), porosity: float = 0.6,
                       rmax: float = 10.0, seed: int = 1234, u_in: float = 0.04, tau: float = 0.6,
                       tau_g: float = 0.55, ka: float = 1e-3, kd: float = 1e-5, q_max: float = 1.0,
                       storage: Storage = Storage.F32, zou_he_inlet: bool = True,
-                      mask: Optional[np.ndarray] = None) -> Tuple[m.Parameters, ps.Parameters]:
+                      mask: Optional[np.ndarray] = None, collision=None) -> Tuple[m.Parameters, ps.Parameters]:
     """Coupled D3Q19 flow + scalar with Langmuir adsorption through a sphere packing.
 
     Inlet z = 0 (Bottom): Zou-He velocity u_z (engine extension) or, for the
@@ -149,7 +149,7 @@ def packed_bed_scalar(n: Sequence[int] = (192, 192, 384), porosity: float = 0.6,
     if mask is None:
         mask = sphere_pack(n, porosity, rmin, rmax, seed)
     inlet = m.ZouHe(None, [0.0, 0.0, u_in]) if zou_he_inlet else m.BounceBack(1.0, [0.0, 0.0, u_in])
-    mp = m.Parameters(n=list(n), collision_operator=BGK(tau), velocity_set=VelocitySet.D3Q19,
+    mp = m.Parameters(n=list(n), collision_operator=collision or BGK(tau), velocity_set=VelocitySet.D3Q19,
                       initial_density=m.InitialDensity.Uniform(1.0),
                       initial_velocity=m.InitialVelocity.Uniform([0.0, 0.0, 0.0]),
                       boundary_conditions=[(W, m.NoSlip), (E, m.NoSlip), (S, m.NoSlip), (N, m.NoSlip),

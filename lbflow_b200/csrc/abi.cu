@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 
 #include "../../include/lbflow.h"
@@ -252,6 +253,11 @@ struct lbf_domain {
     bool compact = false;         // compacted sweep over a work list on the lean path (in effect)
     int compact_opt = -1;         // -1 = default (FP64 storage only), 0 off, 1 on
     long long z_begin = 0, z_end = 0;   // planes swept (0, 0 = all); a z-slab sweeps its owned planes
+    int sparse_opt = -1;          // fluid-only layout on the lean path: 1 on, 0 off, -1 auto (>= 5 % solid)
+    bool sparse = false;          // the sparse layout is in effect: list = fluid cells, pop planes of Np fluid slots
+    uint32_t* fmask = nullptr;    // sparse: mask word per fluid node
+    uint2* rw = nullptr;          // sparse: row words (fluid bits, first fluid index), plus a sentinel row
+    int rw_w = 0;                 // sparse: words per row
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
     long long nlist = 0;
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
@@ -268,7 +274,7 @@ struct lbf_domain {
         }
         for (int f = 0; f < 6; ++f) dev_free(snap[f], dev);
         for (void* p : {(void*)mask, (void*)dtype, qads, cprev, (void*)c_init_dev, (void*)accum, (void*)res_dev,
-                        (void*)obs, (void*)counts, (void*)err, (void*)list})
+                        (void*)obs, (void*)counts, (void*)err, (void*)list, (void*)fmask, (void*)rw})
             dev_free(p, dev);
         pinned64_free(res_host);
     }
@@ -424,6 +430,79 @@ lbf_status build_list(lbf_domain* D, cudaStream_t s) {
     return st;
 }
 
+// The sparse layout (lean path): the fluid cells in node order, their mask
+// words, the row words, and population planes of fluid slots only.
+lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
+    const long long N = D->N, F = (long long)D->n_fluid;
+    // nothing to sweep, or element offsets of the planes beyond 32 bits: stay dense
+    if (F == 0 || F >= (1ll << 31) || (long long)D->q * ((F + 63) / 64 * 64) >= (1ll << 32)) return LBF_OK;
+    const int nx = (int)D->n[0];
+    const int W = (nx + 31) / 32;
+    const long long nrows = D->n[1] * D->n[2], nw = nrows * W;
+    uint8_t* flag = nullptr;
+    uint32_t *val = nullptr, *flist = nullptr, *bits = nullptr, *cnt = nullptr, *off = nullptr;
+    int* nsel = nullptr;
+    void* tmp = nullptr;
+    size_t tb1 = 0, tb2 = 0;
+    lbf_status st = LBF_OK;
+    cudaError_t e = dev_alloc((void**)&flag, N, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&val, N * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&nsel, sizeof(int), D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&bits, nw * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&cnt, nw * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&off, nw * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&flist, F * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&D->fmask, F * 4, D->dev);
+    if (e == cudaSuccess) e = dev_alloc((void**)&D->rw, (nw + W) * sizeof(uint2), D->dev);
+    if (e == cudaSuccess) {
+        k_fluid_flags<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(D->mask, N, flag, val);
+        k_row_bits<<<(unsigned)((nw + 255) / 256), 256, 0, s>>>(D->mask, nx, nrows, W, bits, cnt);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(nullptr, tb1, val, flag, flist, nsel, (int)N, s);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, cnt, off, (int)nw, s);
+    if (e == cudaSuccess) e = dev_alloc(&tmp, std::max(tb1, tb2), D->dev);
+    if (e == cudaSuccess) e = cub::DeviceSelect::Flagged(tmp, tb1, val, flag, flist, nsel, (int)N, s);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb2, cnt, off, (int)nw, s);
+    if (e == cudaSuccess) {
+        k_row_words<<<(unsigned)((nw + W + 255) / 256), 256, 0, s>>>(bits, off, nw, W, (uint32_t)F, D->rw);
+        k_gather_mask<<<(unsigned)((F + 255) / 256), 256, 0, s>>>(D->mask, flist, F, D->fmask);
+        e = cudaGetLastError();
+    }
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nsel, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && h != F) e = cudaErrorUnknown;
+    dev_free(flag, D->dev); dev_free(val, D->dev); dev_free(nsel, D->dev); dev_free(tmp, D->dev);
+    dev_free(bits, D->dev); dev_free(cnt, D->dev); dev_free(off, D->dev);
+    // population planes of fluid slots only
+    const long long Fp = (F + 63) / 64 * 64;
+    const size_t eb = st_bytes(D->st);
+    void* np[2] = {nullptr, nullptr};
+    if (e == cudaSuccess) e = dev_alloc(&np[0], (size_t)D->q * Fp * eb, D->dev);
+    if (e == cudaSuccess) e = dev_alloc(&np[1], (size_t)D->q * Fp * eb, D->dev);
+    if (e != cudaSuccess) {
+        dev_free(flist, D->dev); dev_free(np[0], D->dev); dev_free(np[1], D->dev);
+        dev_free(D->fmask, D->dev); dev_free(D->rw, D->dev);
+        D->fmask = nullptr; D->rw = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_EDEVICE,
+                    std::string("sparse layout: ") + cudaGetErrorString(e));
+    }
+    const long long old_bytes = 2ll * D->q * D->Np * (long long)eb;
+    dev_free(D->pop[0], D->dev);
+    dev_free(D->pop[1], D->dev);
+    D->pop[0] = np[0];
+    D->pop[1] = np[1];
+    D->Np = Fp;
+    D->bytes += 2ll * D->q * Fp * (long long)eb - old_bytes + F * 8 + (nw + W) * 8;
+    D->list = flist;
+    D->nlist = F;
+    D->rw_w = W;
+    D->sparse = true;
+    return st;
+}
+
 // Node classification + device masks (Lattice::new), run once before init.
 lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaStream_t s) {
     const long long N = D->N;
@@ -484,8 +563,22 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
             CK(cudaMemsetAsync(D->snap[f], 0, b, s));   // solid neighbours read as zero populations
         }
     }
+    if (D->sparse) {             // already laid out (a repeated classification keeps the state)
+        D->prepared = true;
+        return LBF_OK;
+    }
     D->nlist = 0;
     if (D->list) { dev_free(D->list, D->dev); D->list = nullptr; }
+    const bool lean = !D->facebc && !D->scalar && !z_restricted(D);
+    const bool porous = (double)D->n_fluid <= 0.95 * (double)N;
+    if (lean && (D->sparse_opt > 0 || (D->sparse_opt < 0 && porous)) && !D->initialized) {
+        if ((st = build_sparse(D, s))) return st;
+        if (D->sparse) {
+            D->compact = false;
+            D->prepared = true;
+            return LBF_OK;
+        }
+    }
     const bool want = (D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0) && !z_restricted(D);
     D->compact = want;
     if (!D->facebc && !D->scalar && want && N < (1ll << 30) && (st = build_list(D, s))) return st;
@@ -504,6 +597,10 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.inv_nx = 1.0 / (double)D->n[0];
     P.inv_ny = 1.0 / (double)D->n[1];
     P.z0 = (int)zb(D);
+    P.fmask = D->fmask;
+    P.rw = D->rw;
+    P.rw_w = D->rw_w;
+    P.np = D->Np;
     const size_t eb = st_bytes(D->st);
     for (int i = 0; i < D->q; ++i) {
         P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->Np * eb;
@@ -611,8 +708,27 @@ cudaError_t launch_list(lbf_domain* D, const StepParams& P, cudaStream_t s) {
     }
 }
 
+cudaError_t launch_sparse(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    const int coll = D->desc.collision.kind;
+    switch (D->vs) {
+        case LBF_D2Q9:
+            return coll == LBF_BGK ? launch_step_sparse<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, s)
+                 : coll == LBF_TRT ? launch_step_sparse<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, s)
+                                   : launch_step_sparse<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, s);
+        case LBF_D3Q19:
+            return coll == LBF_BGK ? launch_step_sparse<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, s)
+                 : coll == LBF_TRT ? launch_step_sparse<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, s)
+                                   : launch_step_sparse<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, s);
+        default:
+            return coll == LBF_BGK ? launch_step_sparse<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), s)
+                 : coll == LBF_TRT ? launch_step_sparse<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), s)
+                                   : launch_step_sparse<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), s);
+    }
+}
+
 // The bulk sweep, then one face pass per scalar outflow face.
 cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    if (D->sparse) return launch_sparse(D, P, s);
     const bool lean = !D->facebc && !D->scalar && !P.first && !P.observe && !P.face_pass;
     if (D->pipe && lean && can_pipe(D)) {
         cudaError_t e = launch_pipe(D, P, s);
@@ -678,9 +794,15 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     void* pb[12];
     for (int f = 0; f < 6; ++f) { pb[2 * f] = D->pb[f][0]; pb[2 * f + 1] = D->pb[f][1]; }
     Launch L{dim3((unsigned)((D->N + 255) / 256)), dim3(256), s};
-    cudaError_t e = D->vs == LBF_D2Q9 ? launch_init<VS_D2Q9>(D->st, D->scalar, P, I, pb, L)
-                  : D->vs == LBF_D3Q19 ? launch_init<VS_D3Q19>(D->st, D->scalar, P, I, pb, L)
-                                       : launch_init<VS_D3Q27>(D->st, D->scalar, P, I, pb, L);
+    cudaError_t e;
+    if (D->sparse)
+        e = D->vs == LBF_D2Q9 ? launch_init_sparse<VS_D2Q9>(D->st, P, I, s)
+          : D->vs == LBF_D3Q19 ? launch_init_sparse<VS_D3Q19>(D->st, P, I, s)
+                               : launch_init_sparse<VS_D3Q27>(D->st, P, I, s);
+    else
+        e = D->vs == LBF_D2Q9 ? launch_init<VS_D2Q9>(D->st, D->scalar, P, I, pb, L)
+          : D->vs == LBF_D3Q19 ? launch_init<VS_D3Q19>(D->st, D->scalar, P, I, pb, L)
+                               : launch_init<VS_D3Q27>(D->st, D->scalar, P, I, pb, L);
     if (tmp) {
         cudaStreamSynchronize(s);
         dev_free(tmp, D->dev);
@@ -1095,6 +1217,10 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
             if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_COMPACT before lbf_domain_init");
             D->compact_opt = value != 0 ? 1 : 0;
             return LBF_OK;
+        case LBF_OPT_SPARSE:
+            if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_SPARSE before lbf_domain_init");
+            D->sparse_opt = value != 0 ? 1 : 0;
+            return LBF_OK;
         case LBF_OPT_Z_BEGIN:
         case LBF_OPT_Z_END:
             if (D->prepared) return fail(LBF_ESTATE, "set the swept z planes before lbf_domain_init");
@@ -1116,6 +1242,7 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
         case LBF_OPT_PIPE: *value = (D->pipe && can_pipe(D)) ? 1 : 0; return LBF_OK;
         case LBF_OPT_PIPE_STAGES: *value = D->pipe_stages; return LBF_OK;
         case LBF_OPT_COMPACT: *value = (D->compact && D->list) ? 1 : 0; return LBF_OK;
+        case LBF_OPT_SPARSE: *value = D->sparse ? 1 : 0; return LBF_OK;
         case LBF_OPT_Z_BEGIN: *value = zb(D); return LBF_OK;
         case LBF_OPT_Z_END: *value = ze(D); return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
@@ -1189,7 +1316,7 @@ struct lbf_batch {
     };
     struct Group {
         int vs = 0, coll = 0, st = 0;
-        bool facebc = false;
+        bool facebc = false, sparse = false;
         std::vector<int> mem;          // indices into members
         void* tab = nullptr;           // KParams<vs>[n] (device)
         BatchState* bs = nullptr;      // device state
@@ -1322,9 +1449,12 @@ lbf_status phase_align(lbf_domain* D, const lbf_batch::Member& m, int k, cudaStr
 
 cudaError_t batch_launch_step(const lbf_batch::Group& g, int j, cudaStream_t s) {
     switch (g.vs) {
-        case LBF_D2Q9: return launch_step_batch<VS_D2Q9>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
-        case LBF_D3Q19: return launch_step_batch<VS_D3Q19>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
-        default: return launch_step_batch<VS_D3Q27>(g.coll, g.st, g.facebc, g.tab, g.bs, g.blk, j, g.nblocks, s);
+        case LBF_D2Q9:
+            return launch_step_batch<VS_D2Q9>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, j, g.nblocks, s);
+        case LBF_D3Q19:
+            return launch_step_batch<VS_D3Q19>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, j, g.nblocks, s);
+        default:
+            return launch_step_batch<VS_D3Q27>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, j, g.nblocks, s);
     }
 }
 cudaError_t batch_launch_finalize(const lbf_batch::Group& g, cudaStream_t s) {
@@ -1360,11 +1490,12 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         const int coll = D->desc.collision.kind;
         lbf_batch::Group* g = nullptr;
         for (auto& x : b->groups)
-            if (x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc) g = &x;
+            if (x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc && x.sparse == D->sparse)
+                g = &x;
         if (!g) {
             b->groups.emplace_back();
             g = &b->groups.back();
-            g->vs = D->vs; g->coll = coll; g->st = D->st; g->facebc = D->facebc;
+            g->vs = D->vs; g->coll = coll; g->st = D->st; g->facebc = D->facebc; g->sparse = D->sparse;
         }
         g->mem.push_back((int)i);
     }
@@ -1400,7 +1531,8 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
             x.d = D->d;
             x.has_scalar = D->scalar ? 1 : 0;
             for (int i = 0; i < 3; ++i) x.tol[i] = m.tol[i];
-            const long long nb = (D->N + BATCH_BLOCK - 1) / BATCH_BLOCK;
+            const long long units = D->sparse ? D->nlist : D->N;   // fluid nodes, or all nodes
+            const long long nb = (units + BATCH_BLOCK - 1) / BATCH_BLOCK;
             blk.insert(blk.end(), (size_t)nb, (int)p);
         }
         if (blk.size() >= (1ull << 31)) return fail(LBF_EUNSUPPORTED, "batch group larger than 2^31 blocks");

@@ -150,6 +150,71 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
     }
 }
 
+// initialize_nodes for the sparse (fluid-only) layout: fluid node k (cell
+// list[k]) gets f = f_eq(rho0, u0) at population index k; the residual moments
+// stay indexed by cell.
+template <int VS, int ST>
+__global__ void k_init_sparse(const StepParams P, const InitParams I0) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= P.nlist) return;
+    const long long cell = P.list[k];
+    const double rho = I0.rho_field ? I0.rho_field[cell] : I0.rho0;
+    double u[3] = {I0.u0[0], I0.u0[1], I0.u0[2]};
+    if (I0.u_field)
+        for (int a = 0; a < D; ++a) u[a] = I0.u_field[cell * D + a];
+    double uu = 0.0;
+    for (int a = 0; a < D; ++a) uu += u[a] * u[a];
+    sfor<Q>([&](auto Ii) {
+        constexpr int i = Ii;
+        const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
+        S::st(const_cast<void*>(P.srcp[i]), (int)k, R(fe));
+    });
+    if (P.mom_prev) {
+        R* mp = (R*)P.mom_prev;
+        mp[cell] = R(rho);
+        for (int a = 0; a < D; ++a) mp[(1 + a) * P.N + cell] = R(u[a]);
+    }
+}
+
+// ---- set-up of the sparse layout --------------------------------------------------
+// flag[cell] = fluid, val[cell] = cell (input of the fluid-list selection)
+static __global__ void k_fluid_flags(const uint32_t* mask, long long N, uint8_t* flag, uint32_t* val) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= N) return;
+    flag[c] = (mask[c] & M_SOLID) ? 0 : 1;
+    val[c] = (uint32_t)c;
+}
+// fluid bits of word w of each row (rows = ny * nz, W words of 32 x each) and their counts
+static __global__ void k_row_bits(const uint32_t* mask, int nx, long long nrows, int W, uint32_t* bits,
+                                  uint32_t* cnt) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j >= nrows * W) return;
+    const long long row = j / W;
+    const int w = (int)(j - row * W);
+    uint32_t b = 0;
+    for (int t = 0; t < 32; ++t) {
+        const int x = 32 * w + t;
+        if (x < nx && !(mask[row * nx + x] & M_SOLID)) b |= 1u << t;
+    }
+    bits[j] = b;
+    cnt[j] = __popc(b);
+}
+// row words {bits, first fluid index at or after the word}, then a sentinel row
+static __global__ void k_row_words(const uint32_t* bits, const uint32_t* off, long long n, int W, uint32_t total,
+                                   uint2* rw) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j < n) rw[j] = make_uint2(bits[j], off[j]);
+    else if (j < n + W) rw[j] = make_uint2(0u, total);
+}
+static __global__ void k_gather_mask(const uint32_t* mask, const uint32_t* list, long long n, uint32_t* out) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k < n) out[k] = mask[list[k]];
+}
+
 // Sum the NSLOT partials of each accumulator; out[k] = sqrt(sum) for residuals
 // or the plain sum for inventories; clears the partials for the next use.
 static __global__ void k_finalize(double* accum, int nacc, int take_sqrt, double* out) {

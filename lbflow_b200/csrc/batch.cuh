@@ -27,9 +27,10 @@ struct BatchState {
 // domains of the group share the velocity set VS, the collision, the storage
 // and the explicit-face flag.  `tab` holds one KParams<VS> per domain (laid out
 // for an even time step), `blk` maps each of the nblocks blocks to its domain.
+// `sparse`: the group's domains use the fluid-only layout.
 template <int VS>
-cudaError_t launch_step_batch(int coll, int st, bool facebc, const void* tab, const BatchState* bs, const int* blk,
-                              int j, unsigned nblocks, cudaStream_t s);
+cudaError_t launch_step_batch(int coll, int st, bool facebc, bool sparse, const void* tab, const BatchState* bs,
+                              const int* blk, int j, unsigned nblocks, cudaStream_t s);
 // Residuals + stop rule + t0 += k for each of the n domains of a group.
 template <int VS>
 cudaError_t launch_batch_finalize(const void* tab, BatchState* bs, int n, cudaStream_t s);

@@ -11,7 +11,8 @@
 // stopped, or whose next step is past its last one, costs its blocks one load
 // and an early exit.  The per-node work is the same code as the single-domain
 // sweep (process_cell), so a domain computes the same values alone and in a
-// batch.  Scalar domains are not batched.
+// batch.  Scalar domains are not batched.  Domains in the sparse (fluid-only)
+// layout form their own groups, swept by k_step_batch_sparse.
 #pragma once
 
 #include "batch.cuh"
@@ -125,6 +126,22 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
     if (P.residual) block_accumulate<5>(racc, P.accum);
 }
 
+// The batched sweep over domains in the sparse (fluid-only) layout: block b
+// covers 256 fluid nodes of domain blk[b], in fluid order.
+template <int VS, int COLL, int ST>
+__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
+    k_step_batch_sparse(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs,
+                        const int* __restrict__ blk, int j) {
+    __shared__ KParams<VS> Ps;
+    const int e = blk[blockIdx.x];
+    const long long t = bs[e].t0 + j;
+    if (bs[e].done_t >= 0 || t > bs[e].last_t) return;   // uniform over the block
+    batch_params<VS, COLL>(Ps, tab, e, t, bs[e].k);
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    sparse_node<VS, COLL, ST>(Ps, (long long)(blockIdx.x - bs[e].block0) * BATCH_BLOCK + threadIdx.x, racc);
+    if (Ps.residual) block_accumulate<5>(racc, Ps.accum);
+}
+
 // One block of 32 threads per domain: residuals of the chunk's last step (its
 // residual step), the stop rule of lbf_domain_run, and t0 += k.
 template <int VS>
@@ -175,17 +192,23 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
 }
 
 #define LBF_BATCH_CASE(C_, S_, FB_)                                                                \
-    if (coll == C_ && st == S_ && facebc == FB_) {                                                 \
+    if (coll == C_ && st == S_ && facebc == FB_ && !sparse) {                                      \
         k_step_batch<VS, C_, S_, FB_><<<nblocks, BATCH_BLOCK, 0, s>>>((const KParams<VS>*)tab, bs, blk, j); \
         return cudaGetLastError();                                                                 \
     }
-#define LBF_BATCH_ST(C_, S_) LBF_BATCH_CASE(C_, S_, false) LBF_BATCH_CASE(C_, S_, true)
+#define LBF_BATCH_SPARSE_CASE(C_, S_)                                                              \
+    if (coll == C_ && st == S_ && sparse) {                                                        \
+        k_step_batch_sparse<VS, C_, S_><<<nblocks, BATCH_BLOCK, 0, s>>>((const KParams<VS>*)tab, bs, blk, j); \
+        return cudaGetLastError();                                                                 \
+    }
+#define LBF_BATCH_ST(C_, S_) LBF_BATCH_CASE(C_, S_, false) LBF_BATCH_CASE(C_, S_, true) LBF_BATCH_SPARSE_CASE(C_, S_)
 #define LBF_BATCH_COLL(C_) LBF_BATCH_ST(C_, ST_F64) LBF_BATCH_ST(C_, ST_F32) LBF_BATCH_ST(C_, ST_F16) LBF_BATCH_ST(C_, ST_BF16)
 
 #define LBF_INSTANTIATE_BATCH(VS_)                                                                 \
     template <>                                                                                    \
-    cudaError_t launch_step_batch<VS_>(int coll, int st, bool facebc, const void* tab, const BatchState* bs, \
-                                       const int* blk, int j, unsigned nblocks, cudaStream_t s) {   \
+    cudaError_t launch_step_batch<VS_>(int coll, int st, bool facebc, bool sparse, const void* tab,     \
+                                       const BatchState* bs, const int* blk, int j, unsigned nblocks, \
+                                       cudaStream_t s) {                                            \
         constexpr int VS = VS_;                                                                    \
         if (nblocks == 0) return cudaSuccess;                                                      \
         LBF_BATCH_COLL(COLL_BGK) LBF_BATCH_COLL(COLL_TRT) LBF_BATCH_COLL(COLL_MRT)                 \

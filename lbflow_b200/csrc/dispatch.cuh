@@ -102,6 +102,20 @@ cudaError_t launch_list_st(const KParams<VS>& kp, cudaStream_t stream) {
     return cudaGetLastError();
 }
 
+// Sparse (fluid-only) sweep (lean path).
+template <int VS, int COLL>
+cudaError_t launch_step_sparse(int st, const StepParams& base, const double* lam, cudaStream_t stream);
+
+template <int VS, int COLL, int ST>
+cudaError_t launch_sparse_st(const KParams<VS>& kp, cudaStream_t stream) {
+    const unsigned blocks = (unsigned)((kp.nlist + 255) / 256);
+    if (blocks == 0) return cudaSuccess;
+    k_step_sparse<VS, COLL, ST><<<blocks, 256, 0, stream>>>(kp);
+    return cudaGetLastError();
+}
+template <int VS>
+cudaError_t launch_init_sparse(int st, const StepParams& P, const InitParams& I, cudaStream_t s);
+
 // One translation unit per (velocity set, collision) instantiates the step kernels.
 template <int VS, int COLL>
 cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const StepParams& base, const double* lam,
@@ -130,6 +144,20 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
             case ST_F32: return launch_list_st<VS_, COLL_, ST_F32>(kp, stream);                        \
             case ST_F16: return launch_list_st<VS_, COLL_, ST_F16>(kp, stream);                        \
             case ST_BF16: return launch_list_st<VS_, COLL_, ST_BF16>(kp, stream);                      \
+            default: return cudaErrorInvalidValue;                                                     \
+        }                                                                                              \
+    }                                                                                                  \
+    template <>                                                                                        \
+    cudaError_t launch_step_sparse<VS_, COLL_>(int st, const StepParams& base, const double* lam,       \
+                                               cudaStream_t stream) {                                  \
+        KParams<VS_> kp;                                                                               \
+        static_cast<StepParams&>(kp) = base;                                                           \
+        fill_lam(kp, lam);                                                                             \
+        switch (st) {                                                                                  \
+            case ST_F64: return launch_sparse_st<VS_, COLL_, ST_F64>(kp, stream);                      \
+            case ST_F32: return launch_sparse_st<VS_, COLL_, ST_F32>(kp, stream);                      \
+            case ST_F16: return launch_sparse_st<VS_, COLL_, ST_F16>(kp, stream);                      \
+            case ST_BF16: return launch_sparse_st<VS_, COLL_, ST_BF16>(kp, stream);                    \
             default: return cudaErrorInvalidValue;                                                     \
         }                                                                                              \
     }                                                                                                  \
@@ -177,6 +205,19 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
                 case ST_BF16: k_init<VS, ST_BF16, false><<<L.grid, L.block, 0, L.stream>>>(P, I, pb[0], pb[1], pb[2], pb[3], pb[4], pb[5], pb[6], pb[7], pb[8], pb[9], pb[10], pb[11]); break; \
                 default: return cudaErrorInvalidValue;                                                 \
             }                                                                                          \
+        }                                                                                              \
+        return cudaGetLastError();                                                                     \
+    }                                                                                                  \
+    template <>                                                                                        \
+    cudaError_t launch_init_sparse<VS_>(int st, const StepParams& P, const InitParams& I, cudaStream_t s) { \
+        const unsigned nb = (unsigned)((P.nlist + 255) / 256);                                         \
+        if (nb == 0) return cudaSuccess;                                                               \
+        switch (st) {                                                                                  \
+            case ST_F64: k_init_sparse<VS_, ST_F64><<<nb, 256, 0, s>>>(P, I); break;                   \
+            case ST_F32: k_init_sparse<VS_, ST_F32><<<nb, 256, 0, s>>>(P, I); break;                   \
+            case ST_F16: k_init_sparse<VS_, ST_F16><<<nb, 256, 0, s>>>(P, I); break;                   \
+            case ST_BF16: k_init_sparse<VS_, ST_BF16><<<nb, 256, 0, s>>>(P, I); break;                 \
+            default: return cudaErrorInvalidValue;                                                     \
         }                                                                                              \
         return cudaGetLastError();                                                                     \
     }                                                                                                  \

@@ -91,6 +91,12 @@ struct StepParams {
     long long nlist;
     double inv_nx, inv_ny;    // 1/nx, 1/ny for index -> coordinate conversion
     int z0, zpad;             // first z plane of the dense sweep (slab domains sweep [z0, z0 + gridDim.z))
+    // sparse layout (fluid nodes only, see k_step_sparse): list = fluid node cells,
+    // nlist = fluid count, fmask = mask word per fluid node, rw = row words
+    const uint32_t* fmask;
+    const uint2* rw;
+    int rw_w, rw_pad;
+    long long np;             // population plane stride in elements (planes of one buffer are np apart)
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -155,14 +161,22 @@ struct Store<ST_F32> {
     __device__ static __forceinline__ R cvt(T v) { return v; }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
 };
+// FP16 holds h_i * 2^14: at low Mach numbers h_i is 1e-7..1e-4, below FP16's
+// smallest normal number (6.1e-5), where the subnormal spacing (6e-8) would cost
+// most of the signal; scaled, every |h| > 3.7e-9 is a normal number with 11
+// significant bits, and |h| < 4 (it is below 1 for any physical state) stays
+// finite.  The scale is a power of two, so scaling itself is exact.
+constexpr float F16_SCALE = 16384.0f, F16_UNSCALE = 1.0f / 16384.0f;
 template <>
 struct Store<ST_F16> {
     using T = __half;
     using R = float;
     static constexpr bool DEV = true;
-    __device__ static __forceinline__ R ld(const void* p, int o) { return __half2float(((const T*)p)[o]); }
-    __device__ static __forceinline__ R cvt(T v) { return __half2float(v); }
-    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v); }
+    __device__ static __forceinline__ R ld(const void* p, int o) {
+        return __half2float(((const T*)p)[o]) * F16_UNSCALE;
+    }
+    __device__ static __forceinline__ R cvt(T v) { return __half2float(v) * F16_UNSCALE; }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v * F16_SCALE); }
 };
 template <>
 struct Store<ST_BF16> {
@@ -755,6 +769,28 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
                 if constexpr (i != ib) S::st(P.dstp[ib], cell, vb);
             }
         });
+    } else if constexpr (VS == VS_D3Q27) {
+        // population-space MRT, f* = f - Lambda (f - f_eq) (+ the Guo source in physics
+        // mode): only the Q deviations e = f - f_eq (+ s/2) stay live through the
+        // Q x Q product, and f_eq_i is re-evaluated when row i is stored, so that FP64
+        // fits the register budget.  With e_j = d_j + s_j / 2:
+        // f_i - sum_j L_ij d_j + s_i - sum_j L_ij s_j / 2 = feq_i + e_i + s_i / 2 - sum_j L_ij e_j
+        const bool src = force && P.compat == COMPAT_PHYSICS;
+        R e[Q];
+        sfor<Q>([&](auto I) {
+            constexpr int i = I;
+            R v = f[i] - eq_i<L, DEV, R>(i, rho, dr, u, uu);
+            if (src) v += R(0.5) * guo_i<L, R>(i, u, F);
+            e[i] = v;
+        });
+        sfor<Q>([&](auto I) {
+            constexpr int i = I;
+            R acc = R(0);
+            sfor<Q>([&](auto J) { acc += lam_at<VS, R>(P, i * Q + J) * e[J]; });
+            R v = eq_i<L, DEV, R>(i, rho, dr, u, uu) + e[i] - acc;
+            if (src) v += R(0.5) * guo_i<L, R>(i, u, F);
+            S::st(P.dstp[i], cell, v);
+        });
     } else {
         R fe[Q];
         sfor<Q>([&](auto I) { fe[I] = eq_i<L, DEV, R>(I, rho, dr, u, uu); });
@@ -806,10 +842,12 @@ constexpr long long WAIT_LIMIT = 1ll << 22;
 // Everything a fluid node does after its populations were pulled: face BCs,
 // moments, residual/observe/face-layer outputs, collision + store, and the
 // scalar step.  Shared by the single-pass sweep and the pipelined sweep.
+// `pidx` is the index of the node's populations in the planes: the node index
+// for the dense layouts, the fluid-node index for the sparse layout.
 template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
-__device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
-                                             typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                             typename Store<ST>::R* gg, double (&racc)[5]) {
+__device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                                typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                                typename Store<ST>::R* gg, double (&racc)[5], long long pidx) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
@@ -901,7 +939,7 @@ __device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g,
         // ---- equilibrium + collision --------------------------------------------
         R uu = R(0);
         sfor<D>([&](auto A) { uu += u[A] * u[A]; });
-        collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, g.cell);
+        collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, pidx);
 
         if constexpr (SCALAR) {
             // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
@@ -934,6 +972,13 @@ __device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g,
             }
         }
     }
+}
+
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                             typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                             typename Store<ST>::R* gg, double (&racc)[5]) {
+    process_cell_at<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc, g.cell);
 }
 
 // =================================================================== the step
@@ -1312,6 +1357,93 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
         }
     }
     if (P.residual) block_accumulate<5>(racc, P.accum);
+}
+
+// =================================================================== sparse sweep
+// The lean path (periodic / no-slip faces, no scalar) over a fluid-only layout:
+// the population planes hold the fluid nodes only, in node order (x fastest), so
+// a porous medium moves no solid bytes and every lane updates a fluid node.
+// Thread k updates fluid node k (cell list[k], link bits fmask[k]).  The pull
+// source (x', y', z') = (x, y, z) - c_i, when fluid, is located through the row
+// words of its row (y', z'): word w holds the fluid bits of x in [32w, 32w + 32)
+// (.x) and the fluid index of the first fluid node at or after x = 32w (.y).
+// With p = .y + popc(.x & bits below x), the fluid nodes of that row before x,
+// the three directions sharing the row read idx(x - 1) = p - 1, idx(x) = p and
+// idx(x + 1) = p + (bit x of the row); the periodic wrap in x (x' = nx - 1 from
+// x = 0, x' = 0 from x = nx - 1) reads the first index of the next row, or of
+// the row.  A sentinel row after the last holds .y = number of fluid nodes.
+// Linked directions (solid source, or a folded no-slip wall) read the node's own
+// f*[ibar], as the dense sweeps do.
+// One fluid node of the sparse sweep (k64 = its fluid index; lanes past the
+// last fluid node only take part in the block reduction).
+template <int VS, int COLL, int ST>
+__device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64, double (&racc)[5]) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    const bool valid = k64 < P.nlist;
+    const int k = valid ? (int)k64 : (int)(P.nlist - 1);
+    Geo g;
+    g.cell = (int)P.list[k];
+    {
+        auto divq = [](int n, int d, double inv) {
+            int q = (int)((double)n * inv);
+            q -= ((long long)q * d > n);
+            q += ((long long)(q + 1) * d <= n);
+            return q;
+        };
+        const int row = divq(g.cell, P.nx, P.inv_nx);
+        g.x = g.cell - row * P.nx;
+        g.z = divq(row, P.ny, P.inv_ny);
+        g.y = row - g.z * P.ny;
+    }
+    g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+    g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+    g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+    g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+    g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+    g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+    const uint32_t mk = P.fmask[k];
+    if (!valid) return;
+    R f[Q];
+    if (P.first) {
+        sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
+    } else {
+        const int W = P.rw_w;
+        const int w = g.x >> 5, b = g.x & 31;
+        const unsigned below = (1u << b) - 1u;
+        const int row = g.y + P.ny * g.z;
+        sfor<Q>([&](auto I) {
+            constexpr int i = I, ib = L::qbar(i);
+            constexpr int cx = L::c(i, 0), cy = L::c(i, 1), cz = D == 3 ? L::c(i, 2) : 0;
+            int idx;
+            if constexpr (cy == 0 && cz == 0) {
+                if constexpr (cx == 0) idx = k;
+                else if constexpr (cx == 1) idx = g.x == 0 ? (int)P.rw[(long long)(row + 1) * W].y - 1 : k - 1;
+                else idx = g.x == P.nx - 1 ? (int)P.rw[(long long)row * W].y : k + 1;
+            } else {
+                const int ys = cy > 0 ? g.ym : (cy < 0 ? g.yp : g.y);
+                const int zs = cz > 0 ? g.zm : (cz < 0 ? g.zp : g.z);
+                const long long r2 = (long long)ys + (long long)P.ny * zs;
+                const uint2 v = P.rw[r2 * W + w];
+                const int p = (int)v.y + __popc(v.x & below);
+                if constexpr (cx == 0) idx = p;
+                else if constexpr (cx == 1) idx = g.x == 0 ? (int)P.rw[(r2 + 1) * W].y - 1 : p - 1;
+                else idx = g.x == P.nx - 1 ? (int)P.rw[r2 * W].y : p + (int)((v.x >> b) & 1u);
+            }
+            const bool lk = (mk >> ib) & 1u;
+            f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
+        });
+    }
+    process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, k);
+}
+
+template <int VS, int COLL, int ST>
+__global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) k_step_sparse(const KParams<VS> P) {
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    sparse_node<VS, COLL, ST>(P, blockIdx.x * (long long)blockDim.x + threadIdx.x, racc);
+    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
 }
 
 // =================================================================== z-slab halos

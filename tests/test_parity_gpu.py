@@ -335,18 +335,66 @@ def test_staged_and_unstaged_sweeps_agree(Domain, storage):
     mask = cases.sphere_pack([32, 20, 16], 0.75, 2.0, 3.5, seed=13)
     p = cases.porous_channel_d3q19([32, 20, 16], mask=mask, force=1e-5, storage=storage)
     out = []
-    for pipe, stage, compact in ((1, 0, 0), (0, 1, 0), (0, 0, 0), (0, 0, 1)):
+    for pipe, stage, compact, sparse in ((1, 0, 0, 0), (0, 1, 0, 0), (0, 0, 0, 0), (0, 0, 1, 0), (0, 0, 0, 1)):
         with Domain(p) as gd:
             gd.set_option(_abi.LBF_OPT_PIPE, pipe)
             gd.set_option(_abi.LBF_OPT_STAGE, stage)
             gd.set_option(_abi.LBF_OPT_COMPACT, compact)
+            gd.set_option(_abi.LBF_OPT_SPARSE, sparse)
             assert gd.get_option(_abi.LBF_OPT_PIPE) == pipe
             assert gd.get_option(_abi.LBF_OPT_STAGE) == stage
             gd.init().step(60, residual_interval=7)
+            assert gd.get_option(_abi.LBF_OPT_SPARSE) == sparse
             out.append(gd.moments() + (gd.residuals()[0],))
     for o in out[1:]:
         assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
         assert np.allclose(out[0][3], o[3], rtol=1e-12, atol=0)
+
+
+def _lean_cases():
+    n2 = [40, 26]
+    m2 = np.zeros(n2[0] * n2[1], np.uint8).reshape(n2[1], n2[0])
+    m2[8:14, 10:17] = 1
+    m2[15:22, 25:31] = 1
+    d2q9 = m.Parameters(n=n2, collision_operator=TRT.from_magic(0.8, 0.25), velocity_set=VelocitySet.D2Q9,
+                        force=[1e-5, 0.0], boundary_conditions=[(W, m.Periodic), (E, m.Periodic), (S, m.NoSlip),
+                                                                (N, m.NoSlip)],
+                        node_types=m.NodeTypes.FromArray(m2.ravel()))
+    mask = cases.sphere_pack([33, 18, 14], 0.7, 1.5, 3.0, seed=17)   # nx = 33: rows span two words
+    d3q19 = cases.porous_channel_d3q19([33, 18, 14], mask=mask, force=1e-5, storage=Storage.F64)
+    mask27 = cases.sphere_pack([20, 12, 16], 0.8, 1.5, 2.5, seed=19)
+    d3q27 = m.Parameters(n=[20, 12, 16], collision_operator=BGK(0.75), velocity_set=VelocitySet.D3Q27,
+                         force=[1e-5, 0.0, 1e-6],
+                         boundary_conditions=[(f, m.Periodic if f in (W, E, B, T) else m.NoSlip)
+                                              for f in (W, E, S, N, B, T)],
+                         node_types=m.NodeTypes.FromArray(mask27))
+    return {"d2q9": d2q9, "d3q19": d3q19, "d3q27": d3q27}
+
+
+@pytest.mark.parametrize("name", ["d2q9", "d3q19", "d3q27"])
+def test_sparse_layout_matches_oracle(Domain, name):
+    """The fluid-only layout: fields vs the oracle, residuals, inventory, and the
+    moments observed before the first step."""
+    p = _lean_cases()[name]
+    steps = 150
+    od = oracle_run(p, steps)
+    ro, uo, _ = od.observe()
+    with Domain(p) as gd:
+        gd.set_option(_abi.LBF_OPT_SPARSE, 1)
+        gd.init()
+        assert gd.get_option(_abi.LBF_OPT_SPARSE) == 1
+        r0, u0, _ = gd.moments()
+        gd.step(steps - 1, residual_interval=1).step(1, residual_interval=1)
+        rg, ug, _ = gd.moments()
+        res, t = gd.residuals()
+        inv = gd.inventory()
+        cls, _ = gd.node_class()
+    fl = (cls & _abi.LBF_CLASS_SOLID) == 0
+    ro0, uo0, _ = oracle_run(p, 0).observe()      # rho = 1, u = F / 2 (the force shift)
+    assert rel(r0[fl], ro0[fl]) <= TOL64 and rel(u0[fl], uo0[fl]) <= TOL64
+    assert rel(rg[fl], ro[fl]) <= TOL64 and rel(ug[fl], uo[fl]) <= TOL64
+    assert t == steps - 1 and np.allclose(res, od.residuals(), rtol=1e-7, atol=1e-15)
+    assert np.allclose(inv, od.inventory(), rtol=1e-12)
 
 
 @pytest.mark.parametrize("storage,tol", [(Storage.F16DEV, 3e-2), (Storage.BF16DEV, 2e-1)])
