@@ -344,6 +344,7 @@ def run_serve(args, rank, world, local_rank):
     with Clocks(local_rank) as clk:
         rb = serve.serve_batched(reqs, max_steps=args.max_steps, residual_interval=args.chunk)
     sb = serve.summary(rb)
+    sb["host_times"] = getattr(serve.serve_batched, "host_times", None)
     ss = None
     if not args.no_sequential:
         ss = serve.summary(serve.serve_sequential(reqs, max_steps=args.max_steps, residual_interval=args.chunk))

@@ -258,6 +258,7 @@ struct lbf_domain {
     uint32_t* fmask = nullptr;    // sparse: mask word per fluid node
     uint2* rw = nullptr;          // sparse: row words (fluid bits, first fluid index), plus a sentinel row
     int rw_w = 0;                 // sparse: words per row
+    bool sparse_packed = false;   // sparse: list entries hold packed coordinates
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
     long long nlist = 0;
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
@@ -467,6 +468,8 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     if (e == cudaSuccess) {
         k_row_words<<<(unsigned)((nw + W + 255) / 256), 256, 0, s>>>(bits, off, nw, W, (uint32_t)F, D->rw);
         k_gather_mask<<<(unsigned)((F + 255) / 256), 256, 0, s>>>(D->mask, flist, F, D->fmask);
+        D->sparse_packed = D->n[0] <= 2048 && D->n[1] <= 2048 && D->n[2] <= 1024;
+        if (D->sparse_packed) k_pack_xyz<<<(unsigned)((F + 255) / 256), 256, 0, s>>>(flist, F, nx, (int)D->n[1]);
         e = cudaGetLastError();
     }
     int h = 0;
@@ -601,6 +604,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.rw = D->rw;
     P.rw_w = D->rw_w;
     P.np = D->Np;
+    P.packed = D->sparse_packed ? 1 : 0;
     const size_t eb = st_bytes(D->st);
     for (int i = 0; i < D->q; ++i) {
         P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->Np * eb;
@@ -1317,6 +1321,7 @@ struct lbf_batch {
     struct Group {
         int vs = 0, coll = 0, st = 0;
         bool facebc = false, sparse = false;
+        bool solo = false;             // one large member launched with its own single-domain sweep
         std::vector<int> mem;          // indices into members
         void* tab = nullptr;           // KParams<vs>[n] (device)
         BatchState* bs = nullptr;      // device state
@@ -1488,14 +1493,20 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
     for (size_t i = 0; i < b->members.size(); ++i) {
         const lbf_domain* D = b->members[i].D;
         const int coll = D->desc.collision.kind;
+        // a large member runs its own sweep in the graph; its launch parameters are
+        // fixed per chunk step only when k is even (t0 keeps its parity)
+        const long long units = D->sparse ? D->nlist : D->N;
+        const bool solo = b->k % 2 == 0 && units >= SOLO_UNITS && !D->pipe && !D->stage;
         lbf_batch::Group* g = nullptr;
         for (auto& x : b->groups)
-            if (x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc && x.sparse == D->sparse)
+            if (!solo && !x.solo && x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc &&
+                x.sparse == D->sparse)
                 g = &x;
         if (!g) {
             b->groups.emplace_back();
             g = &b->groups.back();
             g->vs = D->vs; g->coll = coll; g->st = D->st; g->facebc = D->facebc; g->sparse = D->sparse;
+            g->solo = solo;
         }
         g->mem.push_back((int)i);
     }
@@ -1532,7 +1543,7 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
             x.has_scalar = D->scalar ? 1 : 0;
             for (int i = 0; i < 3; ++i) x.tol[i] = m.tol[i];
             const long long units = D->sparse ? D->nlist : D->N;   // fluid nodes, or all nodes
-            const long long nb = (units + BATCH_BLOCK - 1) / BATCH_BLOCK;
+            const long long nb = g.solo ? 0 : (units + BATCH_BLOCK - 1) / BATCH_BLOCK;
             blk.insert(blk.end(), (size_t)nb, (int)p);
         }
         if (blk.size() >= (1ull << 31)) return fail(LBF_EUNSUPPORTED, "batch group larger than 2^31 blocks");
@@ -1552,8 +1563,22 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = cudaSuccess;
         for (int j = 0; j < b->k && e == cudaSuccess; ++j)
-            for (auto& g : b->groups)
-                if (e == cudaSuccess) e = batch_launch_step(g, j, b->cap);
+            for (auto& g : b->groups) {
+                if (e != cudaSuccess) break;
+                if (!g.solo) {
+                    e = batch_launch_step(g, j, b->cap);
+                    continue;
+                }
+                lbf_domain* D = b->members[g.mem[0]].D;
+                const long long t = D->t + j;
+                StepParams P;
+                base_params(D, P, t);
+                P.residual = t % b->k == 0 ? 1 : 0;
+                P.write_mom = (t % b->k == 0 || (t + 1) % b->k == 0) ? 1 : 0;
+                P.gate = (const GateView*)g.bs;
+                P.gate_j = j;
+                e = launch_step_any(D, P, b->cap);
+            }
         for (auto& g : b->groups)
             if (e == cudaSuccess) e = batch_launch_finalize(g, b->cap);
         for (auto& g : b->groups)

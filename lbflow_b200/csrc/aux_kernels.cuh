@@ -161,7 +161,10 @@ __global__ void k_init_sparse(const StepParams P, const InitParams I0) {
     constexpr int Q = L::Q, D = L::D;
     const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k >= P.nlist) return;
-    const long long cell = P.list[k];
+    const uint32_t e = P.list[k];
+    const long long cell = P.packed ? (long long)(e & 2047u) +
+                                          (long long)P.nx * ((long long)((e >> 11) & 2047u) + (long long)P.ny * (e >> 22))
+                                    : (long long)e;
     const double rho = I0.rho_field ? I0.rho_field[cell] : I0.rho0;
     double u[3] = {I0.u0[0], I0.u0[1], I0.u0[2]};
     if (I0.u_field)
@@ -213,6 +216,15 @@ static __global__ void k_row_words(const uint32_t* bits, const uint32_t* off, lo
 static __global__ void k_gather_mask(const uint32_t* mask, const uint32_t* list, long long n, uint32_t* out) {
     const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (k < n) out[k] = mask[list[k]];
+}
+// node index -> x | y << 11 | z << 22 (lattices up to 2048 x 2048 x 1024)
+static __global__ void k_pack_xyz(uint32_t* list, long long n, int nx, int ny) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t c = list[k];
+    const uint32_t x = c % (uint32_t)nx, r = c / (uint32_t)nx;
+    const uint32_t y = r % (uint32_t)ny, z = r / (uint32_t)ny;
+    list[k] = x | (y << 11) | (z << 22);
 }
 
 // Sum the NSLOT partials of each accumulator; out[k] = sqrt(sum) for residuals

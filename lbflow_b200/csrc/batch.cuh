@@ -2,6 +2,8 @@
 // batched sweep (kernels in batch_kernels.cuh, instantiated by batch_<vs>.cu).
 #pragma once
 
+#include <cstddef>
+
 #include "kernels.cuh"
 
 namespace lbf {
@@ -36,5 +38,12 @@ template <int VS>
 cudaError_t launch_batch_finalize(const void* tab, BatchState* bs, int n, cudaStream_t s);
 
 constexpr int BATCH_BLOCK = 256;
+static_assert(offsetof(BatchState, t0) == offsetof(GateView, t0) && offsetof(BatchState, last_t) ==
+                  offsetof(GateView, last_t) && offsetof(BatchState, done_t) == offsetof(GateView, done_t),
+              "GateView mirrors the leading fields of BatchState");
+// Members with at least this many nodes (fluid nodes in the sparse layout) run
+// their own single-domain sweep inside the chunk graph: they fill the GPU alone,
+// and the single-domain kernels read their parameters from the constant bank.
+constexpr long long SOLO_UNITS = 1ll << 19;
 
 }  // namespace lbf

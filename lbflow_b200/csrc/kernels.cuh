@@ -70,6 +70,13 @@ struct SFaceBC {
     double u[3];
 };
 
+// The leading fields of a batch member's device state (BatchState): a single-
+// domain sweep launched inside a batch's chunk graph skips its launch when the
+// domain has stopped or the step (t0 + gate_j) is past its last one.
+struct GateView {
+    long long t0, last_t, block0, done_t;
+};
+
 struct StepParams {
     int nx, ny, nz, dims;
     long long N;
@@ -97,6 +104,9 @@ struct StepParams {
     const uint2* rw;
     int rw_w, rw_pad;
     long long np;             // population plane stride in elements (planes of one buffer are np apart)
+    const GateView* gate;     // batch member state, or null outside batches
+    int gate_j;               // chunk step of this launch
+    int packed;               // sparse list entries are x | y << 11 | z << 22 (else node indices)
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -839,6 +849,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
 }
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
+// A launch that belongs to a stopped batch member, or to a step past its last
+// one, does nothing (uniform over the grid).
+__device__ __forceinline__ bool gated_off(const StepParams& P) {
+    if (!P.gate) return false;
+    const GateView g = *P.gate;
+    return g.done_t >= 0 || g.t0 + P.gate_j > g.last_t;
+}
+
 // Everything a fluid node does after its populations were pulled: face BCs,
 // moments, residual/observe/face-layer outputs, collision + store, and the
 // scalar step.  Shared by the single-pass sweep and the pipelined sweep.
@@ -1000,6 +1018,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
     using R = typename S::R;
     using T = typename S::T;
     constexpr int Q = L::Q, D = L::D;
+    if (gated_off(P)) return;
 
     Geo g;
     bool inside;
@@ -1159,6 +1178,7 @@ __global__ void __launch_bounds__(256, ST == ST_F64 ? 2 : 4) k_step_list(const K
     using S = Store<ST>;
     using R = typename S::R;
     constexpr int Q = L::Q, D = L::D;
+    if (gated_off(P)) return;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const bool valid = t < P.nlist;
     const uint32_t e = valid ? P.list[t] : 0u;
@@ -1385,14 +1405,20 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
     const bool valid = k64 < P.nlist;
     const int k = valid ? (int)k64 : (int)(P.nlist - 1);
     Geo g;
-    g.cell = (int)P.list[k];
-    {
+    const uint32_t e = P.list[k];
+    if (P.packed) {   // coordinates packed at set-up: no division
+        g.x = (int)(e & 2047u);
+        g.y = (int)((e >> 11) & 2047u);
+        g.z = (int)(e >> 22);
+        g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+    } else {
         auto divq = [](int n, int d, double inv) {
             int q = (int)((double)n * inv);
             q -= ((long long)q * d > n);
             q += ((long long)(q + 1) * d <= n);
             return q;
         };
+        g.cell = (int)e;
         const int row = divq(g.cell, P.nx, P.inv_nx);
         g.x = g.cell - row * P.nx;
         g.z = divq(row, P.ny, P.inv_ny);
@@ -1441,6 +1467,7 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
 
 template <int VS, int COLL, int ST>
 __global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) k_step_sparse(const KParams<VS> P) {
+    if (gated_off(P)) return;
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     sparse_node<VS, COLL, ST>(P, blockIdx.x * (long long)blockDim.x + threadIdx.x, racc);
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);

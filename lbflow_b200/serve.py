@@ -115,6 +115,7 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
     live = {}
     ready = []                 # (request, initialised domain) waiting for admission
     s_batch, s_init = torch.cuda.Stream(), torch.cuda.Stream()
+    host = {"create_s": 0.0, "step_enqueue_s": 0.0, "poll_wait_s": 0.0, "moments_s": 0.0, "chunks": 0}
     with Batch(budget_bytes, residual_interval) as batch:
         budget = batch.info()["budget"]
         used = 0
@@ -123,7 +124,8 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
 
         def create(limit_s):
             nonlocal i, used
-            t_end = time.perf_counter() + limit_s
+            t_start = time.perf_counter()
+            t_end = t_start + limit_s
             while i < len(pending) and pending[i].arrival <= _now(t0) and used + pending[i].est_bytes <= budget:
                 r = pending[i]
                 dom = Domain(r.params)
@@ -134,6 +136,7 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
                 if time.perf_counter() > t_end:
                     break
             s_init.synchronize()
+            host["create_s"] += time.perf_counter() - t_start
 
         while i < len(pending) or live or ready:
             if not live and not ready:
@@ -146,15 +149,24 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
                 batch.admit(dom, max_it, tol_density=math.inf, tol_velocity=tol_velocity, tol_scalar=math.inf)
                 live[dom.h.value] = (r, dom, _now(t0))
             ready.clear()
+            t1 = time.perf_counter()
             batch.step(chunks_per_poll, s_batch)
+            host["step_enqueue_s"] += time.perf_counter() - t1
+            host["chunks"] += chunks_per_poll
             create(create_ms / 1e3)          # overlaps the chunk on the GPU
-            for dom, status in batch.poll(wait=True):
+            t1 = time.perf_counter()
+            done = batch.poll(wait=True)
+            host["poll_wait_s"] += time.perf_counter() - t1
+            for dom, status in done:
                 r, _, start = live.pop(dom.h.value)
+                t1 = time.perf_counter()
                 dom.moments(s_batch)             # the fields reach the host
+                host["moments_s"] += time.perf_counter() - t1
                 records.append(Record(r.rid, r.kind, int(np.prod(r.params.n[: r.params.dim])), r.arrival, start,
                                       _now(t0), dom.time_step, status))
                 used -= r.est_bytes
                 dom.close()
+    serve_batched.host_times = host
     return records
 
 

@@ -181,3 +181,47 @@ def test_batch_many_small_domains(env):
             rho = d.moments()[0]
         assert got[i][0] == 100 and got[i][1] == 2
         assert rel(got[i][2], rho) <= 1e-5
+
+
+def test_batch_large_members_run_their_own_sweep(env):
+    """Members above SOLO_UNITS (2^19 nodes, or fluid nodes in the sparse layout)
+    run the single-domain sweep inside the chunk graph, gated by their batch state;
+    small members share the batched launches.  Same fields and steps as alone."""
+    Domain, Batch, _ = env
+    mask = cases.sphere_pack([96, 96, 96], 0.7, 3.0, 6.0, seed=4)
+    mix = [
+        (cases.porous_channel_d3q19([96, 96, 96], mask=mask, force=1e-5, storage=Storage.F32), 1e-5),  # sparse, solo
+        (cases.cavity_d2q9(768, 0.6, 0.1, Storage.F32), 1e-5),                                        # dense faces, solo
+        (cases.cavity_d2q9(12, 0.8, 0.01, Storage.F64), 1e-12),                                       # small, converges
+        (cases.cavity_d2q9(40, 0.6, 0.1, Storage.F32), 1e-5),                                         # small
+    ]
+    max_it = 300
+    alone = []
+    for p, _ in mix:
+        with Domain(p) as d:
+            d.init()
+            steps = d.run(max_it, K, 1e-7, 1e-7, 1e-7)
+            rho, u, _ = d.moments()
+            cls, _ = d.node_class()
+        alone.append((steps, rho, u, (cls & _abi.LBF_CLASS_SOLID) == 0))
+    with Batch(0, K) as batch:
+        live = {}
+        for i, (p, _) in enumerate(mix):
+            d = Domain(p).init()
+            batch.admit(d, max_it, 1e-7, 1e-7, 1e-7)
+            live[d.h.value] = i
+        got = {}
+        for _ in range(200):
+            if not live:
+                break
+            batch.step(2)
+            for dom, status in batch.poll(wait=True):
+                rho, u, _ = dom.moments()
+                got[live.pop(dom.h.value)] = (dom.time_step, rho, u)
+                dom.close()
+    assert not live
+    for i, (p, tol) in enumerate(mix):
+        steps, rho, u, fl = alone[i]
+        gs, gr, gu = got[i]
+        assert gs == steps, (i, gs, steps)
+        assert rel(gr[fl], rho[fl]) <= tol and rel(gu[fl], u[fl]) <= tol, i
