@@ -15,8 +15,9 @@
 // whose neighbour is solid by the node's own reflected value (src/lib.rs:154-165),
 // applies the face BCs in order (src/momentum/bc.rs:29-149), and only then
 // collides.  Two population buffers alternate (A/B): each node's Q values are
-// read once and written once per step, and boundary rules keep the exact
-// reference semantics ("streaming scheme").
+// read once and written once per step, and the boundary rules keep the exact
+// reference semantics: wall rules, periodic wrap and asymmetric periodic/wall
+// pairs act on the same post-stream populations as in the reference.
 //
 // The step at t = 0 reads f_0 = f_eq(rho0, u0) from the node itself
 // (Lattice::initialize_nodes, src/momentum/lattice.rs:322-328).

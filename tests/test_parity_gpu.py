@@ -33,8 +33,9 @@ def _report():
     yield
     import json
     import os
-    if os.path.isdir("gpurun_out") and REPORT:
-        with open(os.path.join("gpurun_out", "parity_report.json"), "a") as fh:
+    path = os.environ.get("LBF_PARITY_REPORT")   # optional JSON-lines file of the measured errors
+    if path and REPORT:
+        with open(path, "a") as fh:
             fh.write(json.dumps(REPORT) + "\n")
 
 
