@@ -139,7 +139,7 @@ def load() -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    path = library_path()
+    path = os.environ.get("LBF_LIBRARY") or library_path()   # an alternative build, if given
     if not os.path.exists(path):
         raise ImportError(
             f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
