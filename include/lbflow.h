@@ -239,6 +239,22 @@ lbf_status lbf_domain_time_step(lbf_domain* dom, int64_t* t);
 lbf_status lbf_domain_device_bytes(lbf_domain* dom, int64_t* bytes);
 lbf_status lbf_domain_destroy(lbf_domain* dom);
 
+/* ---- checkpoints ----------------------------------------------------------- */
+/* No counterpart in the reference, which restarts from the CSV fields of a time
+ * step (InitialDensity/InitialVelocity::FromTimeStep, src/momentum/io.rs:358-394):
+ * that restores rho and u only, and the populations restart at equilibrium.  A
+ * checkpoint holds the domain's whole carried state: the populations (and scalar
+ * populations) the next step reads, q_ads and the previous scalar value, the
+ * residual moments, the face layers of the previous step, the time step and the
+ * last residuals; a run resumed from it continues bit for bit.
+ * lbf_domain_checkpoint_bytes: size of the host buffer.  lbf_domain_save copies
+ * the state into it.  lbf_domain_load restores it into a domain created from the
+ * same descriptors and options and initialised (lattice, storage, layout and
+ * scalar set-up are checked: LBF_EINVAL if they differ). */
+lbf_status lbf_domain_checkpoint_bytes(lbf_domain* dom, int64_t* bytes);
+lbf_status lbf_domain_save(lbf_domain* dom, void* host, int64_t cap, void* stream);
+lbf_status lbf_domain_load(lbf_domain* dom, const void* host, int64_t bytes, void* stream);
+
 /* ---- z-slab halos (multi-GPU decomposition) ------------------------------ */
 /* No counterpart in the reference (one process, one lattice).  A lattice split
  * into z-slabs across GPUs runs one domain per slab: its owned planes

@@ -107,6 +107,9 @@ SIGNATURES = {
     "lbf_domain_destroy": (_I32, [_P]),
     "lbf_solve": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _I64, _PD, _PD, _PD, _P]),
     "lbf_inventory_noalloc": (_I32, [_P, _P, _P, _P, _P, _I64, _I32, _P, _P]),
+    "lbf_domain_checkpoint_bytes": (_I32, [_P, _PI64]),
+    "lbf_domain_save": (_I32, [_P, _P, _I64, _P]),
+    "lbf_domain_load": (_I32, [_P, _P, _I64, _P]),
     "lbf_domain_halo_info": (_I32, [_P, _PI32, _PI64, _PI64]),
     "lbf_domain_halo_pack": (_I32, [_P, _I32, _P, _P]),
     "lbf_domain_halo_unpack": (_I32, [_P, _I32, _P, _P]),

@@ -908,6 +908,41 @@ lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream
     return LBF_OK;
 }
 
+// ---- checkpoints --------------------------------------------------------------
+// The state a run carries from one step to the next: the post-collision
+// populations (and scalar populations) the next step reads, the in-place scalar
+// fields, the residual moments of the last residual steps, the face layers of the
+// previous step, and the time step with the last residuals.
+struct CkptHeader {
+    char magic[8];        // "LBFCKPT1"
+    int32_t vs, q, st, d;
+    int64_t N, Np, nlist;
+    int32_t sparse, scalar, ads, nsec;
+    int64_t t, res_step;
+    double res[8];
+    int64_t sec_bytes[32];
+};
+
+struct Section {
+    void* dev;
+    size_t bytes;
+};
+
+std::vector<Section> ckpt_sections(const lbf_domain* D) {
+    std::vector<Section> s;
+    const size_t eb = st_bytes(D->st), rb = rt_bytes(D->st);
+    s.push_back({D->pop[D->t & 1], (size_t)D->q * D->Np * eb});
+    s.push_back({D->scalar ? D->gpop[D->t & 1] : nullptr, D->scalar ? (size_t)D->q * D->Np * rb : 0});
+    s.push_back({D->qads, D->qads ? (size_t)D->N * rb : 0});
+    s.push_back({D->cprev, D->cprev ? (size_t)D->N * rb : 0});
+    for (int k = 0; k < 2; ++k)
+        s.push_back({D->mom[k], D->mom[k] ? (size_t)D->nfields() * D->N * rb : 0});
+    for (int f = 0; f < 6; ++f)
+        for (int k = 0; k < 2; ++k)
+            s.push_back({D->pb[f][k], D->pb[f][k] ? (size_t)2 * (D->d + 1) * D->pb_plane[f] * rb : 0});
+    return s;
+}
+
 }  // namespace
 
 // Lets the other translation units of the library report through lbf_last_error().
@@ -1259,6 +1294,83 @@ lbf_status lbf_domain_destroy(lbf_domain* D) {
         if (D->last_stream) cudaStreamSynchronize(D->last_stream);
         delete D;
     }
+    return LBF_OK;
+}
+
+lbf_status lbf_domain_checkpoint_bytes(lbf_domain* D, int64_t* bytes) {
+    if (!D || !bytes) return fail(LBF_EINVAL, "null argument");
+    if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
+    int64_t b = sizeof(CkptHeader);
+    for (const Section& s : ckpt_sections(D)) b += (int64_t)s.bytes;
+    *bytes = b;
+    return LBF_OK;
+}
+
+lbf_status lbf_domain_save(lbf_domain* D, void* host, int64_t cap, void* stream) {
+    int64_t need = 0;
+    lbf_status st = lbf_domain_checkpoint_bytes(D, &need);
+    if (st) return st;
+    if (!host || cap < need) return fail(LBF_EINVAL, "checkpoint buffer smaller than lbf_domain_checkpoint_bytes");
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaStreamSynchronize(D->last_stream));
+    const std::vector<Section> secs = ckpt_sections(D);
+    CkptHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, "LBFCKPT1", 8);
+    h.vs = D->vs; h.q = D->q; h.st = D->st; h.d = D->d;
+    h.N = D->N; h.Np = D->Np; h.nlist = D->sparse ? D->nlist : 0;
+    h.sparse = D->sparse ? 1 : 0; h.scalar = D->scalar ? 1 : 0; h.ads = D->qads ? 1 : 0;
+    h.nsec = (int32_t)secs.size();
+    h.t = D->t; h.res_step = D->res_step;
+    for (int i = 0; i < 8; ++i) h.res[i] = D->res_host[i];
+    char* p = (char*)host;
+    for (size_t i = 0; i < secs.size(); ++i) h.sec_bytes[i] = (int64_t)secs[i].bytes;
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    for (const Section& sec : secs) {
+        if (sec.bytes) CK(cudaMemcpyAsync(p, sec.dev, sec.bytes, cudaMemcpyDeviceToHost, s));
+        p += sec.bytes;
+    }
+    CK(cudaStreamSynchronize(s));
+    return LBF_OK;
+}
+
+lbf_status lbf_domain_load(lbf_domain* D, const void* host, int64_t bytes, void* stream) {
+    if (!D || !host) return fail(LBF_EINVAL, "null argument");
+    if (!D->initialized) return fail(LBF_ESTATE, "create and initialise the domain from the same descriptors first");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
+    if (bytes < (int64_t)sizeof(CkptHeader)) return fail(LBF_EINVAL, "not a checkpoint (too short)");
+    CkptHeader h;
+    std::memcpy(&h, host, sizeof(h));
+    if (std::memcmp(h.magic, "LBFCKPT1", 8) != 0) return fail(LBF_EINVAL, "not a checkpoint (bad magic)");
+    if (h.vs != D->vs || h.q != D->q || h.st != D->st || h.N != D->N || h.Np != D->Np ||
+        h.sparse != (D->sparse ? 1 : 0) || (h.sparse && h.nlist != D->nlist) || h.scalar != (D->scalar ? 1 : 0) ||
+        h.ads != (D->qads ? 1 : 0))
+        return fail(LBF_EINVAL, "checkpoint of a different lattice, storage, layout or scalar set-up");
+    lbf_status st;
+    if ((h.sec_bytes[4] || h.sec_bytes[5]) && (st = ensure_mom(D))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaStreamSynchronize(D->last_stream));
+    D->t = h.t;   // the sections of the state buffers follow the checkpoint's parity
+    const std::vector<Section> secs = ckpt_sections(D);
+    if (h.nsec != (int32_t)secs.size()) return fail(LBF_EINVAL, "checkpoint section count differs");
+    int64_t total = sizeof(CkptHeader);
+    for (size_t i = 0; i < secs.size(); ++i) {
+        if (h.sec_bytes[i] != (int64_t)secs[i].bytes && h.sec_bytes[i] != 0)
+            return fail(LBF_EINVAL, "checkpoint section sizes differ");
+        total += h.sec_bytes[i];
+    }
+    if (bytes < total) return fail(LBF_EINVAL, "checkpoint truncated");
+    const char* p = (const char*)host + sizeof(CkptHeader);
+    for (size_t i = 0; i < secs.size(); ++i) {
+        if (h.sec_bytes[i]) CK(cudaMemcpyAsync(secs[i].dev, p, (size_t)h.sec_bytes[i], cudaMemcpyHostToDevice, s));
+        p += h.sec_bytes[i];
+    }
+    CK(cudaStreamSynchronize(s));
+    D->res_step = h.res_step;
+    for (int i = 0; i < 8; ++i) D->res_host[i] = h.res[i];
+    D->last_stream = s;
     return LBF_OK;
 }
 

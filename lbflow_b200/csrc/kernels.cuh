@@ -1398,7 +1398,8 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
 // One fluid node of the sparse sweep (k64 = its fluid index; lanes past the
 // last fluid node only take part in the block reduction).
 template <int VS, int COLL, int ST>
-__device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64, double (&racc)[5]) {
+__device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k64, uint32_t e, uint32_t mk,
+                                               double (&racc)[5]) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
@@ -1406,7 +1407,6 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
     const bool valid = k64 < P.nlist;
     const int k = valid ? (int)k64 : (int)(P.nlist - 1);
     Geo g;
-    const uint32_t e = P.list[k];
     if (P.packed) {   // coordinates packed at set-up: no division
         g.x = (int)(e & 2047u);
         g.y = (int)((e >> 11) & 2047u);
@@ -1431,7 +1431,6 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
     g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
     g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
     g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
-    const uint32_t mk = P.fmask[k];
     if (!valid) return;
     R f[Q];
     if (P.first) {
@@ -1475,6 +1474,12 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
         else pull(IC<0>{});
     }
     process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, k);
+}
+
+template <int VS, int COLL, int ST>
+__device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64, double (&racc)[5]) {
+    const int k = k64 < P.nlist ? (int)k64 : (int)(P.nlist - 1);
+    sparse_node_at<VS, COLL, ST>(P, k64, P.list[k], P.fmask[k], racc);
 }
 
 template <int VS, int COLL, int ST>

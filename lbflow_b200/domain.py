@@ -141,6 +141,21 @@ class Domain:
         _abi.check(self.lib.lbf_domain_inventory(self.h, _ptr(out), _stream_handle(stream)))
         return out[: 3 + self.d]
 
+    def save(self, path: str, stream=None) -> int:
+        """Write a checkpoint of the carried state (lbf_domain_save); returns its bytes."""
+        n = C.c_int64()
+        _abi.check(self.lib.lbf_domain_checkpoint_bytes(self.h, C.byref(n)))
+        buf = np.empty(n.value, dtype=np.uint8)
+        _abi.check(self.lib.lbf_domain_save(self.h, buf.ctypes.data, n.value, _stream_handle(stream)))
+        buf.tofile(path)
+        return n.value
+
+    def load(self, path: str, stream=None) -> "Domain":
+        """Restore a checkpoint into this (initialised, same-descriptor) domain."""
+        buf = np.fromfile(path, dtype=np.uint8)
+        _abi.check(self.lib.lbf_domain_load(self.h, buf.ctypes.data, buf.size, _stream_handle(stream)))
+        return self
+
     def node_class(self):
         cls = np.zeros(self.N, np.uint32)
         links = np.zeros(self.N, np.uint32)
