@@ -613,6 +613,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     const lbf_collision_desc& c = D->desc.collision;
     P.coll = c.kind; P.compat = D->desc.compat; P.has_force = D->desc.has_force; P.first = t == 0;
     P.tau = c.tau; P.omega = c.kind == LBF_BGK ? 1.0 / c.tau : 0.0; P.op = c.omega_plus; P.om = c.omega_minus;
+    P.bgk_cb = c.kind == LBF_BGK ? 1.0 - 0.5 / c.tau : 0.0;
     for (int k = 0; k < 27; ++k) P.rates[k] = c.relaxation[k];
     for (int a = 0; a < 3; ++a) P.force[a] = D->desc.has_force ? D->desc.force[a] : 0.0;
     fill_face_params(D, P);
@@ -631,6 +632,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
         P.has_scalar = 1;
         P.s_coll = s.collision.kind; P.s_inner = s.inner_boundary_condition; P.s_has_source = s.has_source;
         P.s_tau = s.collision.tau; P.s_omega = s.collision.kind == LBF_BGK ? 1.0 / s.collision.tau : 0.0;
+        P.s_bgk_cb = s.collision.kind == LBF_BGK ? 1.0 - 0.5 / s.collision.tau : 0.0;
         P.s_op = s.collision.omega_plus; P.s_om = s.collision.omega_minus; P.s_source = s.source_value;
         P.s_ads = s.has_adsorption;
         P.ka = s.adsorption_rate; P.kd = s.desorption_rate; P.qmax = s.q_max;

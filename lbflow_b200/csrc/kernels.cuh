@@ -108,6 +108,7 @@ struct StepParams {
     const GateView* gate;     // batch member state, or null outside batches
     int gate_j;               // chunk step of this launch
     int packed;               // sparse list entries are x | y << 11 | z << 22 (else node indices)
+    double bgk_cb, s_bgk_cb;  // 1 - 1/(2 tau) of the momentum and scalar BGK sources, computed once
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
     // [layer 0/1][direction][plane node], compute type
@@ -725,6 +726,18 @@ __device__ __forceinline__ bool scalar_source(const StepParams& P, bool bb, R c_
     return true;
 }
 
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+// Explicitly rounded products and fused multiply-adds: the compiler may not
+// contract them differently in different kernels, so every sweep variant of a
+// step computes the same bits.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // Equilibrium, collision and store of the post-collision populations.  BGK and
 // TRT are evaluated one direction (BGK) or one opposite pair (TRT) at a time
 // and stored at once, so only f[] stays live; MRT needs all moments together.
@@ -740,7 +753,7 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
     constexpr bool DEV = S::DEV;
     if constexpr (COLL == COLL_BGK) {
         const R w1 = R(P.omega), w0 = R(1) - R(P.omega);
-        const R cb = R(1.0 - 0.5 / P.tau);
+        const R cb = R(P.bgk_cb);
         sfor<Q>([&](auto I) {
             constexpr int i = I;
             R v = w0 * f[i] + w1 * eq_i<L, DEV, R>(i, rho, dr, u, uu);
@@ -754,7 +767,14 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
         // for an opposite pair (i, ibar), c_ibar.u = -c_i.u: the symmetric part of the
         // equilibrium is w (base + rho (4.5 (c.u)^2 - 1.5 u.u)), the antisymmetric 3 w rho c.u
         const R base = DEV ? dr : rho;
-        const R ruu = R(1.5) * rho * uu;
+        const R ruu = mul_rn(mul_rn(R(1.5), rho), uu);
+        // f_i - wp (f+_i - feq+_i) - wm (f-_i - feq-_i) in affine form:
+        // f*_i = a f_i + b f_ibar + wp feq+_i + wm feq-_i, f*_ibar = a f_ibar + b f_i + wp feq+_i - wm feq-_i,
+        // a = 1 - (wp + wm) / 2, b = (wm - wp) / 2; the per-node factors k2, k0, k1 and their
+        // products with each weight are shared by every pair of that weight
+        const R a = fma_rn(R(-0.5), add_rn(wp, wm), R(1)), bb = mul_rn(R(0.5), add_rn(wm, -wp));
+        const R k2 = mul_rn(wp, mul_rn(R(4.5), rho)), k0 = mul_rn(wp, add_rn(base, -ruu));
+        const R k1 = mul_rn(wm, mul_rn(R(3), rho));
         sfor<Q>([&](auto I) {
             constexpr int i = I, ib = L::qbar(i);
             if constexpr (i <= ib) {
@@ -765,12 +785,10 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
                     else if constexpr (c == -1) cu -= u[A];
                 });
                 const R wi = R(L::w(i));
-                const R fep = wi * (base + R(4.5) * rho * cu * cu - ruu);
-                const R fem = wi * R(3) * rho * cu;
-                const R fp = R(0.5) * (f[i] + f[ib]);
-                const R fm = R(0.5) * (f[i] - f[ib]);
-                R vi = f[i] - wp * (fp - fep) - wm * (fm - fem);
-                R vb = f[ib] - wp * (fp - fep) - wm * (-fm - -fem);
+                const R sym = fma_rn(mul_rn(wi, k2), mul_rn(cu, cu), mul_rn(wi, k0));   // wp feq+_i
+                const R asym = mul_rn(mul_rn(wi, k1), cu);                           // wm feq-_i
+                R vi = fma_rn(a, f[i], fma_rn(bb, f[ib], add_rn(sym, asym)));
+                R vb = fma_rn(a, f[ib], fma_rn(bb, f[i], add_rn(sym, -asym)));
                 if (src) {
                     const R si = guo_i<L, R>(i, u, F), sb = guo_i<L, R>(ib, u, F);
                     vi += cp * R(0.5) * (si + sb) + cm * R(0.5) * (si - sb);
@@ -850,6 +868,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
 }
 constexpr long long WAIT_LIMIT = 1ll << 22;
 
+
 // A launch that belongs to a stopped batch member, or to a step past its last
 // one, does nothing (uniform over the grid).
 __device__ __forceinline__ bool gated_off(const StepParams& P) {
@@ -881,7 +900,7 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
     R drho = R(0);
     sfor<Q>([&](auto I) { drho += f[I]; });
     const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
-    const R inv_rho = R(1) / rho;
+    const R inv_rho = rcp_rn(rho);   // correctly rounded: the same value as 1 / rho
     R u[3] = {R(0), R(0), R(0)};
     sfor<D>([&](auto A) {
         R s = R(0);
@@ -968,7 +987,7 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
                 const R w1 = R(P.s_omega), w0 = R(1) - R(P.s_omega);
                 R src;
                 const bool has = scalar_source<R>(P, bb, cval, q, true, src);
-                const R cb = R(1.0 - 0.5 / P.s_tau);
+                const R cb = R(P.s_bgk_cb);
                 sfor<Q>([&](auto I) {
                     R v = w0 * gg[I] + w1 * ge[I];
                     if (has) v += cb * R(L::w(I)) * src;
