@@ -1471,17 +1471,18 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
                 if constexpr (cy == 0 && cz == 0) {
                     if constexpr (cx == 0) idx = k;
                     else if constexpr (cx == 1)
-                        idx = (wrap && g.x == 0) ? (int)P.rw[(long long)(row + 1) * W].y - 1 : k - 1;
-                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[(long long)row * W].y : k + 1;
+                        idx = (wrap && g.x == 0) ? (int)P.rw[((unsigned)row + 1u) * (unsigned)W].y - 1 : k - 1;
+                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[(unsigned)row * (unsigned)W].y : k + 1;
                 } else {
                     const int ys = cy > 0 ? g.ym : (cy < 0 ? g.yp : g.y);
                     const int zs = cz > 0 ? g.zm : (cz < 0 ? g.zp : g.z);
-                    const long long r2 = (long long)ys + (long long)P.ny * zs;
-                    const uint2 v = P.rw[r2 * W + w];
+                    // row-word indices stay below (rows + 1) * W <= N / 32 + 2 rows + 1 < 2^32
+                    const unsigned r2 = (unsigned)ys + (unsigned)P.ny * (unsigned)zs;
+                    const uint2 v = P.rw[r2 * (unsigned)W + (unsigned)w];
                     const int p = (int)v.y + __popc(v.x & below);
                     if constexpr (cx == 0) idx = p;
-                    else if constexpr (cx == 1) idx = (wrap && g.x == 0) ? (int)P.rw[(r2 + 1) * W].y - 1 : p - 1;
-                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[r2 * W].y : p + (int)((v.x >> b) & 1u);
+                    else if constexpr (cx == 1) idx = (wrap && g.x == 0) ? (int)P.rw[(r2 + 1u) * (unsigned)W].y - 1 : p - 1;
+                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[r2 * (unsigned)W].y : p + (int)((v.x >> b) & 1u);
                 }
                 const bool lk = (mk >> ib) & 1u;
                 f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
