@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
     ap.add_argument("--chunk", type=int, default=50, help="serve: residual interval (steps per chunk)")
     ap.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time baseline")
+    ap.add_argument("--seq-plain", action="store_true",
+                    help="serve: also run the one-at-a-time baseline with the plain dense sweep")
     ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
                     help="N > 1: z-slabs of one n x n x (n N) channel with a halo exchange per step, "
                          "or independent replicas")
@@ -348,6 +350,10 @@ def run_serve(args, rank, world, local_rank):
     ss = None
     if not args.no_sequential:
         ss = serve.summary(serve.serve_sequential(reqs, max_steps=args.max_steps, residual_interval=args.chunk))
+    sp = None
+    if args.seq_plain:
+        sp = serve.summary(serve.serve_sequential(reqs, max_steps=args.max_steps, residual_interval=args.chunk,
+                                                  plain=True))
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([sb["seconds"]], device="cuda", dtype=torch.float64)
@@ -368,6 +374,9 @@ def run_serve(args, rank, world, local_rank):
             "batched": sb, "sequential": ss, "clocks": clk.summary()}
     if ss:
         line["speedup_vs_sequential"] = sb["solves_per_s"] / ss["solves_per_s"]
+    if sp:
+        line["sequential_plain"] = sp
+        line["speedup_vs_sequential_plain"] = sb["solves_per_s"] / sp["solves_per_s"]
     print(json.dumps(line), flush=True)
 
 

@@ -114,7 +114,7 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
             constexpr int i = Ii;
             // FP32-compute formats store h = f_eq - w (evaluated in FP64)
             const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
-            S::st(const_cast<void*>(P.srcp[i]), cell, R(fe));
+            S::st(const_cast<void*>(P.srcp[i]), cell, S::sc(R(fe)));
         });
         if constexpr (SCALAR) {
             sfor<Q>([&](auto Ii) {
@@ -174,7 +174,7 @@ __global__ void k_init_sparse(const StepParams P, const InitParams I0) {
     sfor<Q>([&](auto Ii) {
         constexpr int i = Ii;
         const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
-        S::st(const_cast<void*>(P.srcp[i]), (int)k, R(fe));
+        S::st(const_cast<void*>(P.srcp[i]), (int)k, S::sc(R(fe)));
     });
     if (P.mom_prev) {
         R* mp = (R*)P.mom_prev;

@@ -160,6 +160,8 @@ struct Store<ST_F64> {
     using T = double;
     using R = double;
     static constexpr bool DEV = false;
+    __device__ static __forceinline__ R sc(R v) { return v; }
+    __device__ static __forceinline__ R unsc(R v) { return v; }
     __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
@@ -169,6 +171,8 @@ struct Store<ST_F32> {
     using T = float;
     using R = float;
     static constexpr bool DEV = true;
+    __device__ static __forceinline__ R sc(R v) { return v; }
+    __device__ static __forceinline__ R unsc(R v) { return v; }
     __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
@@ -178,23 +182,30 @@ struct Store<ST_F32> {
 // most of the signal; scaled, every |h| > 3.7e-9 is a normal number with 11
 // significant bits, and |h| < 4 (it is below 1 for any physical state) stays
 // finite.  The scale is a power of two, so scaling itself is exact.
+// The step kernels keep the scaled values H = h * 2^14 in registers: ld/cvt/st
+// move H, the moments unscale the sums (sc/unsc), and the collision folds the
+// scale into its per-node factors.  Every rounding commutes with an exact power
+// of two, so the stored bits are those of unscale -> collide -> scale, with 2 x Q
+// fewer multiplies per node.
 constexpr float F16_SCALE = 16384.0f, F16_UNSCALE = 1.0f / 16384.0f;
 template <>
 struct Store<ST_F16> {
     using T = __half;
     using R = float;
     static constexpr bool DEV = true;
-    __device__ static __forceinline__ R ld(const void* p, int o) {
-        return __half2float(((const T*)p)[o]) * F16_UNSCALE;
-    }
-    __device__ static __forceinline__ R cvt(T v) { return __half2float(v) * F16_UNSCALE; }
-    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v * F16_SCALE); }
+    __device__ static __forceinline__ R sc(R v) { return v * F16_SCALE; }
+    __device__ static __forceinline__ R unsc(R v) { return v * F16_UNSCALE; }
+    __device__ static __forceinline__ R ld(const void* p, int o) { return __half2float(((const T*)p)[o]); }
+    __device__ static __forceinline__ R cvt(T v) { return __half2float(v); }
+    __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v); }
 };
 template <>
 struct Store<ST_BF16> {
     using T = __nv_bfloat16;
     using R = float;
     static constexpr bool DEV = true;
+    __device__ static __forceinline__ R sc(R v) { return v; }
+    __device__ static __forceinline__ R unsc(R v) { return v; }
     __device__ static __forceinline__ R ld(const void* p, int o) { return __bfloat162float(((const T*)p)[o]); }
     __device__ static __forceinline__ R cvt(T v) { return __bfloat162float(v); }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2bfloat16_rn(v); }
@@ -574,7 +585,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (leaves<L>(i, F)) {
-                R v = S::ld(P.srcp[i], g.cell);
+                R v = S::unsc(S::ld(P.srcp[i], g.cell));
                 if (kind == BC_BOUNCE_BACK) {
                     R cu = R(0);
 #pragma unroll
@@ -603,7 +614,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
 #pragma unroll
                 for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
                 // with h = f - w: h[ibar] = -h*[i] + 2 w (rho_w (...) - 1)
-                f[L::qbar(i)] = -S::ld(P.srcp[i], g.cell) +
+                f[L::qbar(i)] = -S::unsc(S::ld(P.srcp[i], g.cell)) +
                                 R(2) * R(L::w(i)) * (rw * (R(1) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3)) -
                                                      (S::DEV ? R(1) : R(0)));
             }
@@ -752,8 +763,9 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
     constexpr int Q = L::Q;
     constexpr bool DEV = S::DEV;
     if constexpr (COLL == COLL_BGK) {
-        const R w1 = R(P.omega), w0 = R(1) - R(P.omega);
-        const R cb = R(P.bgk_cb);
+        // f[] and the result are scaled by the storage scale: so are w1 and cb
+        const R w1 = S::sc(R(P.omega)), w0 = R(1) - R(P.omega);
+        const R cb = S::sc(R(P.bgk_cb));
         sfor<Q>([&](auto I) {
             constexpr int i = I;
             R v = w0 * f[i] + w1 * eq_i<L, DEV, R>(i, rho, dr, u, uu);
@@ -763,7 +775,7 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
     } else if constexpr (COLL == COLL_TRT) {
         const R wp = R(P.op), wm = R(P.om);
         const bool src = force && P.compat == COMPAT_PHYSICS;
-        const R cp = R(1.0 - 0.5 * P.op), cm = R(1.0 - 0.5 * P.om);
+        const R cp = S::sc(R(1.0 - 0.5 * P.op)), cm = S::sc(R(1.0 - 0.5 * P.om));
         // for an opposite pair (i, ibar), c_ibar.u = -c_i.u: the symmetric part of the
         // equilibrium is w (base + rho (4.5 (c.u)^2 - 1.5 u.u)), the antisymmetric 3 w rho c.u
         const R base = DEV ? dr : rho;
@@ -773,8 +785,9 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
         // a = 1 - (wp + wm) / 2, b = (wm - wp) / 2; the per-node factors k2, k0, k1 and their
         // products with each weight are shared by every pair of that weight
         const R a = fma_rn(R(-0.5), add_rn(wp, wm), R(1)), bb = mul_rn(R(0.5), add_rn(wm, -wp));
-        const R k2 = mul_rn(wp, mul_rn(R(4.5), rho)), k0 = mul_rn(wp, add_rn(base, -ruu));
-        const R k1 = mul_rn(wm, mul_rn(R(3), rho));
+        // f[] and the results are scaled by the storage scale: so are k2, k0, k1 and cp, cm
+        const R k2 = S::sc(mul_rn(wp, mul_rn(R(4.5), rho))), k0 = S::sc(mul_rn(wp, add_rn(base, -ruu)));
+        const R k1 = S::sc(mul_rn(wm, mul_rn(R(3), rho)));
         sfor<Q>([&](auto I) {
             constexpr int i = I, ib = L::qbar(i);
             if constexpr (i <= ib) {
@@ -808,7 +821,7 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
         R e[Q];
         sfor<Q>([&](auto I) {
             constexpr int i = I;
-            R v = f[i] - eq_i<L, DEV, R>(i, rho, dr, u, uu);
+            R v = S::unsc(f[i]) - eq_i<L, DEV, R>(i, rho, dr, u, uu);
             if (src) v += R(0.5) * guo_i<L, R>(i, u, F);
             e[i] = v;
         });
@@ -818,13 +831,14 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
             sfor<Q>([&](auto J) { acc += lam_at<VS, R>(P, i * Q + J) * e[J]; });
             R v = eq_i<L, DEV, R>(i, rho, dr, u, uu) + e[i] - acc;
             if (src) v += R(0.5) * guo_i<L, R>(i, u, F);
-            S::st(P.dstp[i], cell, v);
+            S::st(P.dstp[i], cell, S::sc(v));
         });
     } else {
         R fe[Q];
         sfor<Q>([&](auto I) { fe[I] = eq_i<L, DEV, R>(I, rho, dr, u, uu); });
+        sfor<Q>([&](auto I) { f[I] = S::unsc(f[I]); });
         collide<VS, COLL, DEV, R>(P, f, fe, rho, dr, u, F, force, P.tau, P.omega, P.op, P.om, P.rates, P.compat);
-        sfor<Q>([&](auto I) { S::st(P.dstp[I], cell, f[I]); });
+        sfor<Q>([&](auto I) { S::st(P.dstp[I], cell, S::sc(f[I])); });
     }
 }
 
@@ -893,12 +907,18 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
     constexpr bool DEV = S::DEV;
     // ---- face boundary conditions ------------------------------------------
     if constexpr (FACEBC) {
-        if (!P.first && (mk & (M_FACE | M_NEAR))) apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+        if (!P.first && (mk & (M_FACE | M_NEAR))) {
+            // the face rules work on unscaled populations
+            sfor<Q>([&](auto I) { f[I] = S::unsc(f[I]); });
+            apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+            sfor<Q>([&](auto I) { f[I] = S::sc(f[I]); });
+        }
     }
 
     // ---- moments (src/momentum/node.rs:418-457) ------------------------------
     R drho = R(0);
     sfor<Q>([&](auto I) { drho += f[I]; });
+    drho = S::unsc(drho);
     const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
     const R inv_rho = rcp_rn(rho);   // correctly rounded: the same value as 1 / rho
     R u[3] = {R(0), R(0), R(0)};
@@ -909,7 +929,7 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
             if constexpr (c == 1) s += f[I];
             else if constexpr (c == -1) s -= f[I];
         });
-        u[A] = s * inv_rho;
+        u[A] = S::unsc(s) * inv_rho;
     });
     R F[3] = {R(P.force[0]), R(P.force[1]), R(P.force[2])};
     const bool force = P.has_force != 0;

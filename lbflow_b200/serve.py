@@ -191,8 +191,12 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
 
 
 def serve_sequential(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
-                     residual_interval: int = 50, stream=None) -> List[Record]:
-    """One solve at a time in arrival order with Domain.run (same stop rule)."""
+                     residual_interval: int = 50, stream=None, plain: bool = False) -> List[Record]:
+    """One solve at a time in arrival order with Domain.run (same stop rule).
+
+    plain=True runs every solve with the dense single-domain sweep (the sparse
+    fluid-only layout off), the plain kernel without any layout choice."""
+    from . import _abi
     max_it = max_steps - 2
     records = []
     t0 = time.perf_counter()
@@ -202,6 +206,8 @@ def serve_sequential(reqs: List[Request], max_steps: int = 2000, tol_velocity: f
             time.sleep(wait)
         start = _now(t0)
         with Domain(r.params) as dom:
+            if plain:
+                dom.set_option(_abi.LBF_OPT_SPARSE, 0)
             dom.init(stream)
             steps = dom.run(max_it, residual_interval, tol_density=math.inf, tol_velocity=tol_velocity,
                             tol_scalar=math.inf, stream=stream)
