@@ -324,12 +324,8 @@ bool mom_kind_ok(const lbf_domain_desc& ds, int vs, int f, std::string& why) {
             for (int a = 0; a < d; ++a) if (a != ax) tang = tang && b.has_velocity[a];
             bool vel = !b.has_density && b.has_velocity[ax] && tang;
             bool prs = b.has_density && !b.has_velocity[ax] && tang;
-            if (vs == LBF_D2Q9 || vs == LBF_D3Q19) {
-                if (vel || prs) return true;
-                why = "Error: Wrong input of Zou & He (1997) boundary conditions.";
-                return false;
-            }
-            why = "Zou-He is built for D2Q9 (reference) and D3Q19 (extension) only";
+            if (vel || prs) return true;
+            why = "Error: Wrong input of Zou & He (1997) boundary conditions.";
             return false;
         }
         default:

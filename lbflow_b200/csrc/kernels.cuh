@@ -525,7 +525,18 @@ __device__ __forceinline__ void zou_he_d2q9(int face, R* f, const FaceBC& b, R o
     }
 }
 
-// D3Q19 Zou-He (engine extension; the reference has none): Hecht & Harting (2010).
+// sum of c_A^2 over the directions with c_ax * sgn = +1 (the unknowns of a face)
+template <class L, int ax, int sgn, int A>
+__host__ __device__ constexpr int zou_he_m() {
+    int m = 0;
+    for (int i = 0; i < L::Q; ++i)
+        if (L::c(i, ax) * sgn == 1) m += L::c(i, A) * L::c(i, A);
+    return m;
+}
+
+// D3Q19 and D3Q27 Zou-He (engine extension; the reference has none): Hecht &
+// Harting (2010), with the transverse correction of each tangential axis shared
+// by all unknowns that move along it.
 template <class L, int F, class R>
 __device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b, R one) {
     constexpr int ax = F / 2;
@@ -547,6 +558,8 @@ __device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b, R one) {
         for (int a = 0; a < 3; ++a) if (a != ax) u[a] = R(b.u[a]);
         u[ax] = R(sgn) * (R(1) - (s0 + R(2) * sout) / rho);
     }
+    // transverse correction N_t = (S_t - 2 rho u_t / 3) / M, M = sum over the
+    // unknowns of c_t^2: 2 for D3Q19 (S_t / 2 - rho u_t / 3), 6 for D3Q27
     R N[3] = {R(0), R(0), R(0)};
     sfor<3>([&](auto A) {
         if constexpr (A != ax) {
@@ -554,7 +567,9 @@ __device__ __forceinline__ void zou_he_3d(R* f, const FaceBC& b, R one) {
             sfor<L::Q>([&](auto I) {
                 if constexpr (L::c(I, ax) == 0 && L::c(I, A) != 0) s += R(L::c(I, A)) * f[I];
             });
-            N[A] = R(0.5) * s - rho * u[A] / R(3);
+            constexpr int M = zou_he_m<L, ax, sgn, A>();
+            if constexpr (M == 2) N[A] = R(0.5) * s - rho * u[A] / R(3);
+            else N[A] = s / R(M) - R(2) * rho * u[A] / R(3 * M);
         }
     });
     sfor<L::Q>([&](auto I) {
@@ -621,7 +636,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
         });
     } else if (kind == BC_ZOU_HE) {
         if constexpr (VS == VS_D2Q9) zou_he_d2q9<R>(F, f, b, S::DEV ? R(1) : R(0));
-        else if constexpr (VS == VS_D3Q19) zou_he_3d<L, F, R>(f, b, S::DEV ? R(1) : R(0));
+        else zou_he_3d<L, F, R>(f, b, S::DEV ? R(1) : R(0));
     }
 }
 

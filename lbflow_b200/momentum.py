@@ -72,8 +72,8 @@ class AntiBounceBack(BoundaryCondition):
 class ZouHe(BoundaryCondition):
     """ZouHe { density: Option<f64>, velocity: Vec<Option<f64>> } (src/momentum/bc.rs:21-24).
 
-    D2Q9 follows src/velocity_set/d2q9.rs:165-245; D3Q19 is an extension of
-    this engine (the reference has no 3-D Zou-He).
+    D2Q9 follows src/velocity_set/d2q9.rs:165-245; D3Q19 and D3Q27 are an
+    extension of this engine (the reference has no 3-D Zou-He).
     """
     density: Optional[float] = None
     velocity: Sequence[Optional[float]] = (None, None, None)

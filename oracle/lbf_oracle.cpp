@@ -396,11 +396,17 @@ bool zou_he_d2q9(int face, Float* f, bool has_rho, Float rho_in, const int* has_
     }
 }
 
-// Zou-He for D3Q19 -- an EXTENSION of this engine: the reference has no 3-D
-// Zou-He (zou_he_bc_computation is None for D3Q19, src/velocity_set.rs:134-135,
-// and calling it panics).  Hecht & Harting (2010), J. Stat. Mech. P01018:
-// rho from the known populations, then f_i = f_ibar + 6 w_i rho (c_i.u)
-// - sum_t c_it N_t for the unknowns, N_t the transverse momentum correction.
+// Zou-He for D3Q19 and D3Q27 -- an EXTENSION of this engine: the reference has
+// no 3-D Zou-He (zou_he_bc_computation is None for D3Q19, src/velocity_set.rs:134-135,
+// and calling it panics; D3Q27 is a placeholder).  Hecht & Harting (2010),
+// J. Stat. Mech. P01018: rho from the known populations, then for the unknowns
+// (c.n = +1, n the inward normal) f_i = f_ibar + 6 w_i rho (c_i.u) - sum_t c_it N_t,
+// N_t the transverse momentum correction.  Requiring the tangential momentum
+// rho u_t gives N_t = (S_t - 2 rho u_t / 3) / M, with S_t = sum over c.n = 0 of
+// c_t f and M = sum over the unknowns of c_t^2 (2 for D3Q19: N_t = S_t / 2 -
+// rho u_t / 3, Hecht & Harting's form; 6 for D3Q27, whose corners take a share
+// of both tangential corrections).  Mass and normal momentum hold for any N_t,
+// since the unknowns' c_t sum to zero.
 // Velocity inlet (density None, all velocities Some) or pressure boundary
 // (density Some, normal velocity None, tangential velocities Some).
 bool zou_he_general(const VS& v, int face, Float* f, bool has_rho, Float rho_in,
@@ -434,11 +440,14 @@ bool zou_he_general(const VS& v, int face, Float* f, bool has_rho, Float rho_in,
     for (int a = 0; a < v.d; ++a) {
         if (a == ax) continue;
         Float s = 0.0;
+        int M = 0;
         for (int i = 0; i < v.q; ++i) {
             int cn = v.c[i][0] * n_in[0] + v.c[i][1] * n_in[1] + v.c[i][2] * n_in[2];
             if (cn == 0) s += f[i] * (Float)v.c[i][a];
+            if (cn == 1) M += v.c[i][a] * v.c[i][a];
         }
-        N[a] = 0.5 * s - rho * u[a] / 3.0;
+        // M = 2: 0.5 s - rho u / 3 exactly (2 rho u / 6 rounds as rho u / 3)
+        N[a] = s / (Float)M - 2.0 * rho * u[a] / (3.0 * (Float)M);
     }
     for (int i = 0; i < v.q; ++i) {
         int cn = v.c[i][0] * n_in[0] + v.c[i][1] * n_in[1] + v.c[i][2] * n_in[2];
@@ -1039,7 +1048,7 @@ int orc_create(const lbf_domain_desc* ds, void** out) {
             double ftest[27];
             for (int i = 0; i < v.q; ++i) ftest[i] = v.w[i];
             bool r = v.id == LBF_D2Q9 ? zou_he_d2q9(F, ftest, D->bc[F].has_density != 0, D->bc[F].density, D->bc[F].has_velocity, D->bc[F].velocity)
-                                      : (v.id == LBF_D3Q19 && zou_he_general(v, F, ftest, D->bc[F].has_density != 0, D->bc[F].density, D->bc[F].has_velocity, D->bc[F].velocity));
+                                      : zou_he_general(v, F, ftest, D->bc[F].has_density != 0, D->bc[F].density, D->bc[F].has_velocity, D->bc[F].velocity);
             if (!r) { delete D; return fail(LBF_EINVAL, "Error: Wrong input of Zou & He (1997) boundary conditions."); }
         }
     }

@@ -237,6 +237,48 @@ def test_tgv_d3q27_f32(Domain):
     compare(Domain, p, 100, tol_u=TOL32_U, tol_rho=TOL32_RHO)
 
 
+def _zou_he_duct(vs, coll, axis, storage=Storage.F64, porous=False):
+    """Duct along `axis` with a Zou-He velocity inlet and a Zou-He pressure outlet
+    (engine extension for the 3-D sets), no-slip side walls."""
+    n = [10, 9, 8]
+    n[axis] = 16
+    u_in = [0.0, 0.0, 0.0]
+    u_in[axis] = 0.03
+    p_out = [0.0, 0.0, 0.0]
+    p_out[axis] = None
+    faces = [(W, E), (S, N), (B, T)]
+    bcs = []
+    for a, (lo, hi) in enumerate(faces):
+        if a == axis:
+            bcs += [(lo, m.ZouHe(None, u_in)), (hi, m.ZouHe(1.0, p_out))]
+        else:
+            bcs += [(lo, m.NoSlip), (hi, m.NoSlip)]
+    mask = cases.sphere_pack(n, 0.85, 1.5, 2.0, seed=11) if porous else None
+    return m.Parameters(n=n, collision_operator=coll, velocity_set=vs, storage=storage,
+                        initial_velocity=m.InitialVelocity.Uniform([0, 0, 0]), boundary_conditions=bcs,
+                        node_types=m.NodeTypes.FromArray(mask) if porous else m.NodeTypes.OnlyFluidNodes)
+
+
+D3Q27_MRT = MRT([1.0] * 4 + [1.25] * 5 + [1.4] * 18)
+
+
+@pytest.mark.parametrize("axis", [0, 2])
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_zou_he_velocity_inlet_pressure_outlet_d3q27(Domain, axis, coll):
+    p = _zou_he_duct(VelocitySet.D3Q27, BGK(0.7) if coll == "bgk" else D3Q27_MRT, axis, porous=axis == 0)
+    compare(Domain, p, 250)
+
+
+def test_zou_he_d3q27_f32(Domain):
+    p = _zou_he_duct(VelocitySet.D3Q27, TRT(1.25, 0.75), 1, storage=Storage.F32)
+    compare(Domain, p, 250, tol_u=TOL32_U, tol_rho=TOL32_RHO)
+
+
+def test_zou_he_velocity_inlet_pressure_outlet_d3q19(Domain):
+    p = _zou_he_duct(VelocitySet.D3Q19, TRT(1.25, 0.75), 1, porous=True)
+    compare(Domain, p, 250)
+
+
 # ------------------------------------------------------------------ passive scalar
 def _scalar_channel(inner, ads=True, coll=None):
     n = [36, 16]
