@@ -107,9 +107,15 @@ template <int VS, int COLL>
 cudaError_t launch_step_sparse(int st, const StepParams& base, const double* lam, cudaStream_t stream);
 
 template <int VS, int COLL, int ST>
-cudaError_t launch_sparse_st(const KParams<VS>& kp, cudaStream_t stream) {
+cudaError_t launch_sparse_st(KParams<VS>& kp, cudaStream_t stream) {
     const unsigned blocks = (unsigned)((kp.nlist + 255) / 256);
     if (blocks == 0) return cudaSuccess;
+    // prefetch distance: one wave, the blocks that the launch bounds keep resident
+    // on every SM (a plain attribute query, also valid during graph capture)
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    kp.pf_blocks = sms * 2 * light_kernel<VS, COLL, ST, false>();
     k_step_sparse<VS, COLL, ST><<<blocks, 256, 0, stream>>>(kp);
     return cudaGetLastError();
 }

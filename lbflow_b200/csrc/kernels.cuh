@@ -103,7 +103,8 @@ struct StepParams {
     // nlist = fluid count, fmask = mask word per fluid node, rw = row words
     const uint32_t* fmask;
     const uint2* rw;
-    int rw_w, rw_pad;
+    int rw_w;
+    int pf_blocks;            // sparse sweep: a block prefetches into L2 what block + pf_blocks reads first (0: off)
     long long np;             // population plane stride in elements (planes of one buffer are np apart)
     const GateView* gate;     // batch member state, or null outside batches
     int gate_j;               // chunk step of this launch
@@ -1537,9 +1538,45 @@ __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64,
     sparse_node_at<VS, COLL, ST>(P, k64, P.list[k], P.fmask[k], racc);
 }
 
+// One bulk prefetch of a global range into L2 (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// A node's first load (its list entry and mask word) would wait on DRAM, and
+// every later load of the node waits for it.  Thread 0 of each block therefore
+// prefetches into L2 the list entries and mask words of the block that starts
+// about one wave later (block + pf_blocks), together with its own slots k0 ..
+// k0 + n - 1 of the planes it pulls from its own rows (rest and +-x, whose sources
+// lie within one slot of those).  A prefetch moves no extra DRAM bytes: the lines
+// are read once either way.
+template <int VS, int ST>
+__device__ __forceinline__ void sparse_prefetch(const KParams<VS>& P) {
+    using L = Lat<VS>;
+    using T = typename Store<ST>::T;
+    if (P.pf_blocks <= 0 || threadIdx.x != 0) return;
+    const long long k0 = ((long long)blockIdx.x + P.pf_blocks) * blockDim.x;
+    if (k0 >= P.nlist) return;
+    const long long n = P.nlist - k0 < (long long)blockDim.x ? P.nlist - k0 : (long long)blockDim.x;
+    auto pf = [](const void* p, long long bytes) {   // 16-byte aligned start, size rounded down to 16
+        const unsigned b = (unsigned)bytes & ~15u;
+        if (b != 0 && ((uintptr_t)p & 15u) == 0) bulk_prefetch_l2(p, b);
+    };
+    pf(P.list + k0, n * 4);
+    pf(P.fmask + k0, n * 4);
+    if (!P.first) {
+        sfor<L::Q>([&](auto I) {
+            constexpr int i = I;
+            if constexpr (L::c(i, 1) == 0 && (L::D == 2 || L::c(i, 2) == 0))
+                pf((const T*)P.srcp[i] + k0, n * (long long)sizeof(T));
+        });
+    }
+}
+
 template <int VS, int COLL, int ST>
 __global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) k_step_sparse(const KParams<VS> P) {
     if (gated_off(P)) return;
+    sparse_prefetch<VS, ST>(P);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     sparse_node<VS, COLL, ST>(P, blockIdx.x * (long long)blockDim.x + threadIdx.x, racc);
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
