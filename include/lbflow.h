@@ -59,7 +59,9 @@ enum {
     LBF_BC_NO_SLIP = 0,
     LBF_BC_BOUNCE_BACK = 1,      /* moving wall: density, velocity          */
     LBF_BC_ANTI_BOUNCE_BACK = 2, /* pressure: density                       */
-    LBF_BC_ZOU_HE = 3,           /* Option<density>, Vec<Option<velocity>>  */
+    LBF_BC_ZOU_HE = 3,           /* Option<density>, Vec<Option<velocity>>;
+                                    D2Q9 as the reference; D3Q19 / D3Q27 velocity
+                                    and pressure faces are an extension         */
     LBF_BC_PERIODIC = 4
 };
 
