@@ -257,6 +257,7 @@ struct lbf_domain {
     bool sparse = false;          // the sparse layout is in effect: list = fluid cells, pop planes of Np fluid slots
     uint32_t* fmask = nullptr;    // sparse: mask word per fluid node
     uint2* rw = nullptr;          // sparse: row words (fluid bits, first fluid index), plus a sentinel row
+    std::vector<long long> zoff;  // sparse: first fluid index of each z plane, then the fluid count
     int rw_w = 0;                 // sparse: words per row
     bool sparse_packed = false;   // sparse: list entries hold packed coordinates
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
@@ -470,8 +471,18 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     }
     int h = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, nsel, sizeof(int), cudaMemcpyDeviceToHost, s);
+    // the first row word of every z plane (and of the sentinel row) holds the
+    // plane's first fluid index
+    std::vector<uint2> zw((size_t)D->n[2] + 1);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2DAsync(zw.data(), sizeof(uint2), D->rw, (size_t)D->n[1] * W * sizeof(uint2), sizeof(uint2),
+                              (size_t)D->n[2] + 1, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e == cudaSuccess && h != F) e = cudaErrorUnknown;
+    if (e == cudaSuccess) {
+        D->zoff.resize(zw.size());
+        for (size_t z = 0; z < zw.size(); ++z) D->zoff[z] = zw[z].y;
+    }
     dev_free(flag, D->dev); dev_free(val, D->dev); dev_free(nsel, D->dev); dev_free(tmp, D->dev);
     dev_free(bits, D->dev); dev_free(cnt, D->dev); dev_free(off, D->dev);
     // population planes of fluid slots only
@@ -568,7 +579,8 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     }
     D->nlist = 0;
     if (D->list) { dev_free(D->list, D->dev); D->list = nullptr; }
-    const bool lean = !D->facebc && !D->scalar && !z_restricted(D);
+    // the sparse sweep also serves z-slabs (it updates the fluid slots of the owned planes)
+    const bool lean = !D->facebc && !D->scalar;
     const bool porous = (double)D->n_fluid <= 0.95 * (double)N;
     if (lean && (D->sparse_opt > 0 || (D->sparse_opt < 0 && porous)) && !D->initialized) {
         if ((st = build_sparse(D, s))) return st;
@@ -593,6 +605,12 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.err = D->err;
     P.list = D->list;
     P.nlist = D->nlist;
+    P.kbeg = 0;
+    P.kend = D->nlist;
+    if (D->sparse && z_restricted(D)) {
+        P.kbeg = D->zoff[(size_t)zb(D)];
+        P.kend = D->zoff[(size_t)ze(D)];
+    }
     P.inv_nx = 1.0 / (double)D->n[0];
     P.inv_ny = 1.0 / (double)D->n[1];
     P.z0 = (int)zb(D);
@@ -883,13 +901,17 @@ lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream
     const size_t eb = st_bytes(D->st);
     HaloPlanes H{};
     H.plane = plane;
+    // slots of plane z: dense z * plane .. + plane; sparse its fluid nodes
+    const long long first = D->sparse ? D->zoff[(size_t)z] : z * plane;
+    H.count = D->sparse ? D->zoff[(size_t)z + 1] - D->zoff[(size_t)z] : plane;
     for (int i = 0; i < D->q; ++i) {
         int c[3];
         tables_c(D->vs, i, c);
         if (c[2] != want) continue;
-        H.planes[H.nd++] = (char*)D->pop[D->t & 1] + ((size_t)i * D->Np + (size_t)(z * plane)) * eb;
+        H.planes[H.nd++] = (char*)D->pop[D->t & 1] + ((size_t)i * D->Np + (size_t)first) * eb;
     }
-    const long long n = (long long)H.nd * plane;
+    const long long n = (long long)H.nd * H.count;
+    if (n == 0) { D->last_stream = s; return LBF_OK; }
     const unsigned blocks = (unsigned)std::min<long long>((n + 255) / 256, 4 * 148);
     if (eb == 8) {
         if (unpack) k_halo_unpack<double><<<blocks, 256, 0, s>>>(H, (const double*)buf);

@@ -108,7 +108,7 @@ cudaError_t launch_step_sparse(int st, const StepParams& base, const double* lam
 
 template <int VS, int COLL, int ST>
 cudaError_t launch_sparse_st(KParams<VS>& kp, cudaStream_t stream) {
-    const unsigned blocks = (unsigned)((kp.nlist + 255) / 256);
+    const unsigned blocks = (unsigned)((kp.kend - kp.kbeg + 255) / 256);
     if (blocks == 0) return cudaSuccess;
     // prefetch distance: one wave, the blocks that the launch bounds keep resident
     // on every SM (a plain attribute query, also valid during graph capture)

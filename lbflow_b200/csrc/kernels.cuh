@@ -97,6 +97,7 @@ struct StepParams {
     int pipe_stages, pipe_nc; // pipelined sweep: ring stages, consumer warps
     const uint32_t* list;     // compacted sweep: work entries (see k_step_list)
     long long nlist;
+    long long kbeg, kend;     // sparse sweep: the fluid indices it updates (a z-slab: its owned planes)
     double inv_nx, inv_ny;    // 1/nx, 1/ny for index -> coordinate conversion
     int z0, zpad;             // first z plane of the dense sweep (slab domains sweep [z0, z0 + gridDim.z))
     // sparse layout (fluid nodes only, see k_step_sparse): list = fluid node cells,
@@ -1555,9 +1556,11 @@ __device__ __forceinline__ void sparse_prefetch(const KParams<VS>& P) {
     using L = Lat<VS>;
     using T = typename Store<ST>::T;
     if (P.pf_blocks <= 0 || threadIdx.x != 0) return;
-    const long long k0 = ((long long)blockIdx.x + P.pf_blocks) * blockDim.x;
+    // from a multiple of 16 slots (16-byte aligned for every element size)
+    const long long k0 = (P.kbeg + ((long long)blockIdx.x + P.pf_blocks) * blockDim.x) & ~15ll;
     if (k0 >= P.nlist) return;
-    const long long n = P.nlist - k0 < (long long)blockDim.x ? P.nlist - k0 : (long long)blockDim.x;
+    const long long want = (long long)blockDim.x + 16;
+    const long long n = P.nlist - k0 < want ? P.nlist - k0 : want;
     auto pf = [](const void* p, long long bytes) {   // 16-byte aligned start, size rounded down to 16
         const unsigned b = (unsigned)bytes & ~15u;
         if (b != 0 && ((uintptr_t)p & 15u) == 0) bulk_prefetch_l2(p, b);
@@ -1578,7 +1581,8 @@ __global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) 
     if (gated_off(P)) return;
     sparse_prefetch<VS, ST>(P);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sparse_node<VS, COLL, ST>(P, blockIdx.x * (long long)blockDim.x + threadIdx.x, racc);
+    const long long k = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    sparse_node<VS, COLL, ST>(P, k < P.kend ? k : P.nlist, racc);   // nlist: no update
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
 }
 
@@ -1589,25 +1593,31 @@ __global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) 
 // neighbour, and the neighbour's buffer is unpacked into the ghost plane, whose
 // entering directions (c_z = +1 below, -1 above) the next step pulls.
 // planes[k] = element pointer of direction dirs[k] at the plane's first node.
+// In the sparse layout a plane's fluid nodes are `count` consecutive slots (the
+// ghost plane holds the same fluid nodes as the neighbour's boundary plane); the
+// buffer keeps the dense stride `plane` per direction either way.
 struct HaloPlanes {
     void* planes[9];
     int nd;
-    long long plane;   // nodes per plane
+    long long plane;   // buffer elements per direction (nodes per plane)
+    long long count;   // slots copied per direction (plane, or the plane's fluid nodes)
 };
 template <class T>
 __global__ void k_halo_pack(HaloPlanes H, T* buf) {
-    const long long n = (long long)H.nd * H.plane;
+    const long long n = (long long)H.nd * H.count;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i / H.plane);
-        buf[i] = ((const T*)H.planes[k])[i - k * H.plane];
+        const int k = (int)(i / H.count);
+        const long long j = i - k * H.count;
+        buf[k * H.plane + j] = ((const T*)H.planes[k])[j];
     }
 }
 template <class T>
 __global__ void k_halo_unpack(HaloPlanes H, const T* buf) {
-    const long long n = (long long)H.nd * H.plane;
+    const long long n = (long long)H.nd * H.count;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i / H.plane);
-        ((T*)H.planes[k])[i - k * H.plane] = buf[i];
+        const int k = (int)(i / H.count);
+        const long long j = i - k * H.count;
+        ((T*)H.planes[k])[j] = buf[k * H.plane + j];
     }
 }
 

@@ -6,7 +6,9 @@ handed to the neighbours by device copies, and each unpacks into its ghost
 planes (lbf_domain_halo_unpack).  Only ordinary launches on one stream are
 involved; no kernel waits on another.  The owned planes must match the whole
 lattice run as one domain: relative L2 over fluid nodes 1e-12 (FP64 storage),
-1e-6 (FP32).  The multi-process exchange of the same buffers (TorchExchange) is
+1e-6 (FP32).  Lean porous slabs run the sparse sweep (fluid slots of the owned
+planes, halos over each plane's fluid slots); the case with explicit x faces runs
+the dense sweep.  The multi-process exchange of the same buffers (TorchExchange) is
 covered on the CPU by tests/test_slab_cpu.py.
 """
 import os
@@ -54,6 +56,9 @@ def test_slabs_match_whole_lattice_gpu(name, world, storage, tol):
     slabs = [slab.SlabDomain(p, r, world, _Ring(r, world, periodic)) for r in range(world)]
     for s in slabs:
         s.init()
+        # lean porous slabs run the sparse fluid-only sweep over their owned planes,
+        # the others (explicit x faces) the dense sweep
+        assert s.dom.get_option(_abi.LBF_OPT_SPARSE) == (0 if name == "periodic" else 1)
     lib = _abi.load()
     for _ in range(steps):
         for s in slabs:
