@@ -277,6 +277,16 @@ lbf_status lbf_domain_halo_info(lbf_domain* dom, int32_t* ndir, int64_t* plane_n
 lbf_status lbf_domain_halo_pack(lbf_domain* dom, int32_t face, void* dst, void* stream);
 lbf_status lbf_domain_halo_unpack(lbf_domain* dom, int32_t face, const void* src, void* stream);
 
+/* One step of a z-slab domain in two parts, so that the halo exchange overlaps
+ * the interior sweep.  Part 0 updates the owned boundary planes (z_begin and
+ * z_end - 1); lbf_domain_halo_pack then reads them and lbf_domain_halo_unpack
+ * writes the ghost planes that the next step reads, on any stream ordered after
+ * part 0.  Part 1 updates the planes between them, evaluates the residuals of a
+ * residual step (k as in lbf_domain_step) and ends the step.  Parts 0 and 1
+ * alternate (LBF_ESTATE otherwise); other stepping, observing and checkpoint calls
+ * wait for part 1.  Same results as lbf_domain_step. */
+lbf_status lbf_domain_step_part(lbf_domain* dom, int32_t part, int64_t residual_interval, void* stream);
+
 /* ---- FP64 fluid sums with no device allocation --------------------------- */
 /* No counterpart in the reference (whose reductions are rayon sums on the CPU).
  * For callers that cannot allocate device memory when they need the sums: code

@@ -113,6 +113,7 @@ SIGNATURES = {
     "lbf_domain_halo_info": (_I32, [_P, _PI32, _PI64, _PI64]),
     "lbf_domain_halo_pack": (_I32, [_P, _I32, _P, _P]),
     "lbf_domain_halo_unpack": (_I32, [_P, _I32, _P, _P]),
+    "lbf_domain_step_part": (_I32, [_P, _I32, _I64, _P]),
     "lbf_domain_estimate_bytes": (_I32, [C.POINTER(DomainDesc), C.POINTER(ScalarDesc), _PI64]),
     "lbf_batch_create": (_I32, [_I64, _I64, C.POINTER(_P)]),
     "lbf_batch_admit": (_I32, [_P, _P, _I64, _D, _D, _D]),

@@ -245,6 +245,7 @@ struct lbf_domain {
     unsigned long long* counts = nullptr;
     std::vector<double> lam;      // D3Q27 MRT collision matrix
     long long t = 0;
+    bool part_pending = false;    // a split step ran its part 0 (boundary planes) and waits for part 1
     long long res_step = -1;
     int block_x = 0;
     bool stage = false;           // one-shot staged sweep (off: the pipelined sweep supersedes it)
@@ -838,6 +839,7 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
 
 lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s) {
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before stepping");
+    if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     lbf_status st;
     if (k > 0 && (st = ensure_mom(D))) return st;
     for (long long it = 0; it < nsteps; ++it) {
@@ -862,6 +864,7 @@ lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s
 
 lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
+    if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     lbf_status st;
     if (!D->obs && (st = dmalloc(D, (void**)&D->obs, (size_t)D->N * (D->d + 2) * sizeof(double)))) return st;
     StepParams P;
@@ -873,6 +876,21 @@ lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
     cudaError_t e = launch_step_any(D, P, s);
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("observe kernel: ") + cudaGetErrorString(e));
     return LBF_OK;
+}
+
+// The sweep of planes [zlo, zhi) of step P (a z-slab's split step).
+cudaError_t sweep_planes(lbf_domain* D, StepParams P, long long zlo, long long zhi, cudaStream_t s) {
+    if (zlo >= zhi) return cudaSuccess;
+    if (D->sparse) {
+        P.kbeg = D->zoff[(size_t)zlo];
+        P.kend = D->zoff[(size_t)zhi];
+        return launch_sparse(D, P, s);
+    }
+    P.z0 = (int)zlo;
+    const bool stage = D->stage && can_stage(D);
+    const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
+    const dim3 g((unsigned)((D->n[0] + b.x - 1) / b.x), (unsigned)D->n[1], (unsigned)(zhi - zlo));
+    return launch_one(D, P, stage, Launch{g, b, s});
 }
 
 void tables_c(int vs, int i, int* c) {
@@ -899,6 +917,8 @@ lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream
     const long long z = bottom ? (unpack ? z0 - 1 : z0) : (unpack ? z1 : z1 - 1);
     const long long plane = D->n[0] * D->n[1];
     const size_t eb = st_bytes(D->st);
+    // between the parts of a split step, the boundary planes of step t are in buffer (t + 1) & 1
+    const long long tb = D->t + (D->part_pending ? 1 : 0);
     HaloPlanes H{};
     H.plane = plane;
     // slots of plane z: dense z * plane .. + plane; sparse its fluid nodes
@@ -908,7 +928,7 @@ lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream
         int c[3];
         tables_c(D->vs, i, c);
         if (c[2] != want) continue;
-        H.planes[H.nd++] = (char*)D->pop[D->t & 1] + ((size_t)i * D->Np + (size_t)first) * eb;
+        H.planes[H.nd++] = (char*)D->pop[tb & 1] + ((size_t)i * D->Np + (size_t)first) * eb;
     }
     const long long n = (long long)H.nd * H.count;
     if (n == 0) { D->last_stream = s; return LBF_OK; }
@@ -1128,6 +1148,44 @@ lbf_status lbf_domain_step(lbf_domain* D, int64_t nsteps, int64_t residual_inter
     return do_steps(D, nsteps, residual_interval, (cudaStream_t)stream);
 }
 
+lbf_status lbf_domain_step_part(lbf_domain* D, int32_t part, int64_t k, void* stream) {
+    if (!D) return fail(LBF_EINVAL, "null domain");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
+    if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before stepping");
+    if (D->d != 3 || !z_restricted(D)) return fail(LBF_EINVAL, "split steps apply to z-slab domains");
+    if (D->outflow) return fail(LBF_EUNSUPPORTED, "split steps with an outflow face pass are not built");
+    if (part != 0 && part != 1) return fail(LBF_EINVAL, "part must be 0 or 1");
+    if ((part == 1) != D->part_pending) return fail(LBF_ESTATE, part ? "part 1 before part 0" : "part 0 twice");
+    cudaStream_t s = (cudaStream_t)stream;
+    lbf_status st;
+    if (k > 0 && (st = ensure_mom(D))) return st;
+    const long long t = D->t, z0 = zb(D), z1 = ze(D);
+    StepParams P;
+    base_params(D, P, t);
+    P.residual = (k > 0 && t % k == 0) ? 1 : 0;
+    P.write_mom = (k > 0 && (t % k == 0 || (t + 1) % k == 0)) ? 1 : 0;
+    cudaError_t e = cudaSuccess;
+    if (part == 0) {
+        e = sweep_planes(D, P, z0, z0 + 1, s);
+        if (e == cudaSuccess && z1 - 1 > z0) e = sweep_planes(D, P, z1 - 1, z1, s);
+        if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
+        D->part_pending = true;
+    } else {
+        e = sweep_planes(D, P, z0 + 1, z1 - 1, s);
+        if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
+        if (P.residual) {
+            k_finalize<<<1, 32, 0, s>>>(D->accum, 5, 1, D->res_dev);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(D->res_host, D->res_dev, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
+            D->res_step = t;
+        }
+        D->t = t + 1;
+        D->part_pending = false;
+    }
+    D->last_stream = s;
+    return LBF_OK;
+}
+
 lbf_status lbf_domain_run(lbf_domain* D, int64_t max_iterations, int64_t k, double tr, double tu, double tc,
                           int64_t* steps_done, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
@@ -1331,6 +1389,7 @@ lbf_status lbf_domain_save(lbf_domain* D, void* host, int64_t cap, void* stream)
     int64_t need = 0;
     lbf_status st = lbf_domain_checkpoint_bytes(D, &need);
     if (st) return st;
+    if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     if (!host || cap < need) return fail(LBF_EINVAL, "checkpoint buffer smaller than lbf_domain_checkpoint_bytes");
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaStreamSynchronize(D->last_stream));
@@ -1360,6 +1419,7 @@ lbf_status lbf_domain_load(lbf_domain* D, const void* host, int64_t bytes, void*
     if (!D || !host) return fail(LBF_EINVAL, "null argument");
     if (!D->initialized) return fail(LBF_ESTATE, "create and initialise the domain from the same descriptors first");
     if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
+    if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     if (bytes < (int64_t)sizeof(CkptHeader)) return fail(LBF_EINVAL, "not a checkpoint (too short)");
     CkptHeader h;
     std::memcpy(&h, host, sizeof(h));

@@ -200,21 +200,43 @@ class SlabDomain:
         self.dom.init(self._s())
         return self
 
-    def halo(self) -> None:
-        lib, h, s = self.dom.lib, self.dom.h, self._s().cuda_stream
+    def halo(self, stream=None) -> None:
+        """Pack, exchange and unpack the halos on `stream` (default: the domain's)."""
+        import torch
+        st = stream if stream is not None else self._s()
+        lib, h, s = self.dom.lib, self.dom.h, st.cuda_stream
         send_lo, send_hi, recv_lo, recv_hi = self.bufs
         _abi.check(lib.lbf_domain_halo_pack(h, _abi.LBF_BOTTOM, C.c_void_p(send_lo.data_ptr()), C.c_void_p(s)))
         _abi.check(lib.lbf_domain_halo_pack(h, _abi.LBF_TOP, C.c_void_p(send_hi.data_ptr()), C.c_void_p(s)))
-        self.exchange(send_lo, send_hi, recv_lo, recv_hi)
+        with torch.cuda.stream(st):   # the collective orders itself after the packs on this stream
+            self.exchange(send_lo, send_hi, recv_lo, recv_hi)
         if self.exchange.down is not None:
             _abi.check(lib.lbf_domain_halo_unpack(h, _abi.LBF_BOTTOM, C.c_void_p(recv_lo.data_ptr()), C.c_void_p(s)))
         if self.exchange.up is not None:
             _abi.check(lib.lbf_domain_halo_unpack(h, _abi.LBF_TOP, C.c_void_p(recv_hi.data_ptr()), C.c_void_p(s)))
 
-    def step(self, n: int = 1, residual_interval: int = 0) -> "SlabDomain":
+    def step(self, n: int = 1, residual_interval: int = 0, overlap: bool = True) -> "SlabDomain":
+        """n steps with halo exchanges.  overlap: each step runs in two parts
+        (lbf_domain_step_part): the boundary planes, then the interior planes on the
+        domain's stream while the halos are packed, exchanged and unpacked on a
+        second stream; the next step waits for the unpacks."""
+        import torch
+        if not overlap or self.nzl < 3:
+            for _ in range(n):
+                self.dom.step(1, residual_interval, self._s())
+                self.halo()
+            return self
+        s = self._s()
+        if not hasattr(self, "_comm"):
+            self._comm = torch.cuda.Stream()
+        c = self._comm
+        lib, h = self.dom.lib, self.dom.h
         for _ in range(n):
-            self.dom.step(1, residual_interval, self._s())
-            self.halo()
+            _abi.check(lib.lbf_domain_step_part(h, 0, residual_interval, C.c_void_p(s.cuda_stream)))
+            c.wait_stream(s)
+            self.halo(c)
+            _abi.check(lib.lbf_domain_step_part(h, 1, residual_interval, C.c_void_p(s.cuda_stream)))
+            s.wait_stream(c)
         return self
 
     @property
