@@ -108,7 +108,8 @@ def workload_name(args):
 
 def config_of(args, n_fluid, world, sweep):
     return {"workload": workload_name(args), "storage": args.storage, "n_fluid": int(n_fluid),
-            "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N)",
+            "l2": f"inputs larger than L2 (populations 2 x 19 x {SBYTES[args.storage]} B per fluid node, "
+                  f"{2 * 19 * SBYTES[args.storage] * int(n_fluid) / 1e6:.0f} MB)",
             "parallelism": "replicas" if world > 1 else "single", "sweep": sweep}
 
 
@@ -437,7 +438,7 @@ def run_slabs(args, rank, world, local_rank):
                                    f"porosity {args.porosity:g}, periodic x, no-slip y/z)",
                        "storage": args.storage, "n_fluid": int(fluid_all), "parallelism": f"z-slabs x{world}",
                        "halo_bytes_per_step_per_gpu": 2 * halo,
-                       "l2": "inputs larger than L2 (populations 2 x 19 x 4 B x N per GPU)"},
+                       "l2": f"inputs larger than L2 (populations 2 x 19 x {s_b} B per fluid node and GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": profile_traffic(args.storage, args.n), "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
