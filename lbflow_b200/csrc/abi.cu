@@ -1530,6 +1530,11 @@ struct lbf_batch {
     std::vector<Group> groups;
     bool dirty = true;
     cudaStream_t cap = nullptr;        // private stream the chunk graph is captured on
+    // the groups' step chains are captured on side streams forked from cap, so that
+    // the chunk graph runs independent groups (and large members) concurrently
+    static constexpr int NSIDE = 8;
+    cudaStream_t side[NSIDE] = {};
+    cudaEvent_t fork = nullptr, join[NSIDE] = {};
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev = nullptr;
     cudaStream_t last = nullptr;
@@ -1550,6 +1555,11 @@ struct lbf_batch {
         free_groups();
         if (host_buf) cudaFreeHost(host_buf);
         if (ev) cudaEventDestroy(ev);
+        if (fork) cudaEventDestroy(fork);
+        for (int q = 0; q < NSIDE; ++q) {
+            if (join[q]) cudaEventDestroy(join[q]);
+            if (side[q]) cudaStreamDestroy(side[q]);
+        }
         if (cap) cudaStreamDestroy(cap);
     }
 };
@@ -1750,15 +1760,24 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         CK(cudaMemcpy(g.bs, bs.data(), n * sizeof(BatchState), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(g.blk, blk.data(), blk.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
-    // capture one chunk: k steps of every group, finalize, copy the states back
+    // capture one chunk: k steps of every group, finalize, copy the states back.
+    // Groups are independent: each group's chain runs on a side stream forked
+    // from the capture stream.  The large members (solo groups), which fill the
+    // GPU one at a time, share side stream 0 and keep running one after another;
+    // the batched groups of small members take the other side streams in turn and
+    // overlap with them.
     if (!b->members.empty()) {
         CK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = cudaSuccess;
-        for (int j = 0; j < b->k && e == cudaSuccess; ++j)
-            for (auto& g : b->groups) {
-                if (e != cudaSuccess) break;
+        const int ns = (int)std::min<size_t>(lbf_batch::NSIDE, b->groups.size() + 1);
+        cudaError_t e = cudaEventRecord(b->fork, b->cap);
+        for (int q = 0; q < ns && e == cudaSuccess; ++q) e = cudaStreamWaitEvent(b->side[q], b->fork, 0);
+        const int forked = e == cudaSuccess ? ns : 0;
+        for (size_t gi = 0; gi < b->groups.size() && e == cudaSuccess; ++gi) {
+            lbf_batch::Group& g = b->groups[gi];
+            cudaStream_t sg = g.solo || ns == 1 ? b->side[0] : b->side[1 + gi % (size_t)(ns - 1)];
+            for (int j = 0; j < b->k && e == cudaSuccess; ++j) {
                 if (!g.solo) {
-                    e = batch_launch_step(g, j, b->cap);
+                    e = batch_launch_step(g, j, sg);
                     continue;
                 }
                 lbf_domain* D = b->members[g.mem[0]].D;
@@ -1769,13 +1788,18 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
                 P.write_mom = (t % b->k == 0 || (t + 1) % b->k == 0) ? 1 : 0;
                 P.gate = (const GateView*)g.bs;
                 P.gate_j = j;
-                e = launch_step_any(D, P, b->cap);
+                e = launch_step_any(D, P, sg);
             }
-        for (auto& g : b->groups)
-            if (e == cudaSuccess) e = batch_launch_finalize(g, b->cap);
-        for (auto& g : b->groups)
+            if (e == cudaSuccess) e = batch_launch_finalize(g, sg);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(g.host, g.bs, g.mem.size() * sizeof(BatchState), cudaMemcpyDeviceToHost, b->cap);
+                e = cudaMemcpyAsync(g.host, g.bs, g.mem.size() * sizeof(BatchState), cudaMemcpyDeviceToHost, sg);
+        }
+        // every forked side stream rejoins the capture stream, also after an error
+        for (int q = 0; q < forked; ++q) {
+            cudaError_t r = cudaEventRecord(b->join[q], b->side[q]);
+            if (r == cudaSuccess) r = cudaStreamWaitEvent(b->cap, b->join[q], 0);
+            if (e == cudaSuccess) e = r;
+        }
         cudaGraph_t graph = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(b->cap, &graph);
         if (e == cudaSuccess) e = e2;
@@ -1839,6 +1863,11 @@ lbf_status lbf_batch_create(int64_t budget_bytes, int64_t residual_interval, lbf
     b->budget = budget_bytes;
     cudaError_t e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int q = 0; q < lbf_batch::NSIDE && e == cudaSuccess; ++q) {
+        e = cudaStreamCreateWithFlags(&b->side[q], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join[q], cudaEventDisableTiming);
+    }
     if (e != cudaSuccess) { delete b; return fail(LBF_EDEVICE, std::string("batch: ") + cudaGetErrorString(e)); }
     *out = b;
     return LBF_OK;
