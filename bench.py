@@ -5,12 +5,16 @@ porous channel 256^3 (FP32 storage), the headline configuration.
                     [--storage f32|f16dev|bf16dev|f64] [--n 256]
 
 One step = one main_steps over the whole lattice (one fused kernel launch).
-Inputs are resident in HBM (2 x 19 x 4 B x 16.8 M nodes = 2.5 GB of populations,
-far larger than the 126 MB L2, so no flush is needed between steps).  `e2e` is
-the same metric through lbf_solve with host buffers (mask upload, init, K steps
-and the moment download inside the timed region).  Under torchrun each rank
-advances its own copy of the domain (weak scaling, no data-path collective);
-timing is the max over ranks of CUDA-event time on the launching stream.
+Inputs are resident in HBM (2 x 19 x 4 B x 11.7 M fluid nodes = 1.8 GB of
+populations, far larger than the 126 MB L2, so no flush is needed between steps).
+`e2e` is the same metric through lbf_solve with host buffers (node-type upload,
+layout build, init, K steps and the FP64 moment download inside the timed
+region), with the phase split of a second solve.  `accuracy` compares the engine
+(the benchmarked storage, FP32 and FP16 deviations) after --acc-steps steps (100)
+with the FP64 oracle on the same lattice; that oracle run, timed, is the
+`cpu_baseline`.  `same_precision` is the FP64-storage figure.  Under torchrun each
+rank advances its own part (z-slabs, or replicas with --decomp replicas); timing
+is the max over ranks of CUDA-event time on the launching stream.
 
 --impl reference times the CPU oracle (a restatement of the reference's Rust
 step, OpenMP over all host cores) on the same geometry.
@@ -20,7 +24,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -47,13 +50,18 @@ def parse():
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--porosity", type=float, default=0.7, help="target fluid fraction (1.0 = empty channel)")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle run (CPU baseline and accuracy against the oracle)")
+    ap.add_argument("--no-same-precision", action="store_true", help="skip the FP64-storage figure")
     ap.add_argument("--block", type=int, default=0, help="override the x block size")
     ap.add_argument("--sweep", default="auto", choices=["auto", "pipe", "stage", "plain", "sparse"],
                     help="auto: the library's default (the fluid-only sparse layout for porous lean lattices); "
                          "pipelined bulk-copy sweep, one-shot staged sweep, plain dense loads, or sparse")
     ap.add_argument("--stages", type=int, default=0, help="pipeline ring depth (0 = auto)")
     ap.add_argument("--compact", type=int, default=-1, help="1/0: force the fluid work-list sweep on/off")
+    ap.add_argument("--streaming", default="auto", choices=["auto", "pull", "push", "inplace"],
+                    help="streaming scheme of the sparse layout (auto: the library's default)")
+    ap.add_argument("--sround", type=int, default=-1, help="16-bit storage: 1/0 stochastic rounding on/off")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the sweep variant and block size by timing candidates first (untimed)")
     ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy"],
@@ -166,14 +174,20 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def profile_traffic(storage: str, n: int):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"d3q19_trt_porous_step_{storage}.md")
-    if not os.path.exists(path):
-        return None
-    with open(path) as fh:
-        m = re.search(rf"traffic_bytes_per_launch_{n}:\s*([0-9.eE+]+)", fh.read())
-    return float(m.group(1)) if m else None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the
+# headline step kernel, from ncu.  Keyed by (sweep, storage, n).  Provenance of each
+# figure is given beside it; None where no capture exists.
+TRAFFIC_BYTES = {
+    # k_step_sparse<D3Q19, TRT, FP32>: one launch captured at 160^3 (421,772,288 B,
+    # 2,867,096 fluid nodes), scaled to 256^3 by the fluid nodes per launch
+    # (11,743,596); the writes of a single captured launch are under-counted by the
+    # stores still held in L2 when it ends (ncu flushes L2 before each replay).
+    ("sparse", "f32", 256): 1727574994.0,
+}
+
+
+def traffic_of(sweep_key: str, storage: str, n: int):
+    return TRAFFIC_BYTES.get((sweep_key, storage, n))
 
 
 def peaks():
@@ -183,22 +197,6 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def cpu_baseline(args, mask, steps=25):
-    """The oracle on the full lattice for a few main_steps on all host cores."""
-    from lbflow_b200 import momentum as m
-    from oracle import oracle as orc
-    p = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
-    desc, keep = m.to_desc(p)
-    od = orc.Domain(desc, keep=keep).init()
-    od.step(1)
-    t0 = time.perf_counter()
-    od.step(steps)
-    dt = time.perf_counter() - t0
-    return {"value": od.num_fluid * steps / dt / 1e6, "unit": "MLUPS", "cores": orc.num_threads(), "kind": "port",
-            "sample": f"oracle (FP64 CPU restatement) on the same {args.n}^3 lattice, {steps} main_steps after "
-                      f"1 warm-up, {orc.num_threads()} OpenMP threads"}
 
 
 def run_reference(args, rank, world):
@@ -229,23 +227,19 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_engine(args, rank, world, local_rank):
-    import torch
-    import torch.distributed as dist
-    from lbflow_b200 import _abi
-    from lbflow_b200.domain import Domain, solve_arrays
+def sweep_name(dom, _abi):
+    if dom.get_option(_abi.LBF_OPT_SPARSE):
+        sch = dom.get_option(_abi.LBF_OPT_STREAMING)
+        return "sparse fluid-only layout, " + {_abi.LBF_STREAM_PULL: "pull (two buffers)",
+                                               _abi.LBF_STREAM_PUSH: "push (two buffers)",
+                                               _abi.LBF_STREAM_INPLACE: "in place (AA pattern, one buffer)"}[sch]
+    return ("sparse fluid-only layout" if dom.get_option(_abi.LBF_OPT_SPARSE) else
+            "pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
+            "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else
+            "compacted fluid work list" if dom.get_option(_abi.LBF_OPT_COMPACT) else "dense lattice")
 
-    torch.cuda.set_device(local_rank)
-    mask = geometry(args.n, args.seed, args.porosity)
-    p = params_for(args, mask)
-    n_fluid = int(np.count_nonzero(mask == 0))
-    N = mask.size
-    stream = torch.cuda.current_stream()
-    tuned = None
-    if args.autotune:
-        from lbflow_b200 import autotune
-        tuned = autotune.autotune(p, steps=20, cache=None)
-    dom = Domain(p)
+
+def configure(dom, args, _abi, tuned=None):
     if tuned is not None:
         from lbflow_b200 import autotune
         autotune.apply(dom, tuned)
@@ -259,32 +253,175 @@ def run_engine(args, rank, world, local_rank):
         dom.set_option(_abi.LBF_OPT_PIPE_STAGES, args.stages)
     if args.compact >= 0:
         dom.set_option(_abi.LBF_OPT_COMPACT, args.compact)
-    dom.init(stream)
-    sweep = ("sparse fluid-only layout" if dom.get_option(_abi.LBF_OPT_SPARSE) else
-             "pipelined bulk-copy" if dom.get_option(_abi.LBF_OPT_PIPE) else
-             "one-shot staged" if dom.get_option(_abi.LBF_OPT_STAGE) else
-             "compacted fluid work list" if dom.get_option(_abi.LBF_OPT_COMPACT) else "dense lattice")
-    if tuned is not None:
-        sweep += f" (autotuned: {tuned.get('sweep')}, block_x {tuned.get('block_x', 0)})"
+    if args.streaming != "auto":
+        dom.set_option(_abi.LBF_OPT_STREAMING, {"pull": _abi.LBF_STREAM_PULL, "push": _abi.LBF_STREAM_PUSH,
+                                                "inplace": _abi.LBF_STREAM_INPLACE}[args.streaming])
+    if args.sround >= 0:
+        dom.set_option(_abi.LBF_OPT_SROUND, args.sround)
+
+
+def time_steps(dom, steps, warmup, stream, world):
+    """CUDA-event time of `steps` steps after `warmup` untimed ones (max over ranks)."""
+    import torch
+    import torch.distributed as dist
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # the clock sampler starts before the warm-up so that its samples cover the timed steps
-    with Clocks(local_rank) as clk:
-        dom.step(args.warmup, 0, stream)
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-        start.record(stream)
-        dom.step(args.steps, 0, stream)
-        end.record(stream)
-        torch.cuda.synchronize()
+    dom.step(warmup, 0, stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record(stream)
+    dom.step(steps, 0, stream)
+    end.record(stream)
+    torch.cuda.synchronize()
     ms = start.elapsed_time(end)
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
+    return ms
+
+
+def measure_e2e(args, p, n_fluid, N, stream, world):
+    """The same metric through lbf_solve (the C-ABI call with host buffers): node
+    types uploaded, layout built, initialised, K steps, FP64 density and velocity
+    downloaded, all inside the timed region; then the same sequence through the
+    separate ABI calls, timed phase by phase."""
+    import torch
+    import torch.distributed as dist
+    from lbflow_b200.domain import Domain, solve_arrays
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    wall0 = time.perf_counter()
+    solve_arrays(p, args.steps, stream=stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    e_sec = max(t0.elapsed_time(t1) / 1e3, wall)
+    if world > 1:
+        t = torch.tensor([e_sec], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_sec = float(t.item())
+    # phase split of the same work (host clock, device synchronised after each phase)
+    sync = torch.cuda.synchronize
+    split = {}
+    c0 = time.perf_counter()
+    dom = Domain(p)
+    sync(); c1 = time.perf_counter()
+    dom.init(stream)
+    sync(); c2 = time.perf_counter()
+    dom.step(args.steps, 0, stream)
+    sync(); c3 = time.perf_counter()
+    dom.moments(stream)
+    sync(); c4 = time.perf_counter()
+    dom.close()
+    sync(); c5 = time.perf_counter()
+    split = {"create_ms": 1e3 * (c1 - c0), "layout_and_init_ms": 1e3 * (c2 - c1), "steps_ms": 1e3 * (c3 - c2),
+             "download_ms": 1e3 * (c4 - c3), "destroy_ms": 1e3 * (c5 - c4)}
+    return {"value": world * n_fluid * args.steps / e_sec / 1e6, "unit": "MLUPS",
+            "h2d_bytes_per_step": N / args.steps, "d2h_bytes_per_step": N * (1 + 3) * 8 / args.steps,
+            "ms_per_solve": 1e3 * e_sec,
+            "split": split,
+            "note": f"lbf_solve per solve of {args.steps} steps: node-type upload (N x 1 B), layout build, init, "
+                    f"{args.steps} steps, FP64 density + velocity download (N x 32 B); split measured on a second "
+                    "solve through the separate calls"}
+
+
+def accuracy_vs_oracle(args, mask, steps, storages, threads=0):
+    """Engine fields after `steps` steps on the headline lattice, against the FP64
+    oracle after the same steps: relative L2 over fluid nodes of velocity and
+    density, exact node-class agreement.  The oracle's run is timed and returned
+    as the CPU baseline (same lattice, all host threads)."""
+    import torch
+    from lbflow_b200 import _abi
+    from lbflow_b200 import momentum as m
+    from lbflow_b200.domain import Domain
+    from oracle import oracle as orc
+    if threads:
+        orc.set_threads(threads)
+    p64 = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
+    desc, keep = m.to_desc(p64)
+    od = orc.Domain(desc, keep=keep).init()
+    t0 = time.perf_counter()
+    od.step(steps)
+    dt = time.perf_counter() - t0
+    ro, uo, _ = od.observe()
+    cls_o, links_o = od.node_class()
+    fl = (cls_o & _abi.LBF_CLASS_SOLID) == 0
+    base = {"value": od.num_fluid * steps / dt / 1e6, "unit": "MLUPS", "cores": orc.num_threads(), "kind": "port",
+            "sample": f"oracle (FP64 CPU restatement of the reference step) on the same {args.n}^3 lattice, "
+                      f"{steps} main_steps from initialisation, {orc.num_threads()} OpenMP threads "
+                      "(the Rust reference cannot be built here)"}
+    del od
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
+
+    acc = {"steps": steps, "reference": "oracle, FP64", "runs": {}}
+    for st in storages:
+        p = params_for(argparse.Namespace(**{**vars(args), "storage": st}), mask)
+        with Domain(p) as d:
+            d.init().step(steps)
+            rg, ug, _ = d.moments()
+            cls_g, links_g = d.node_class()
+        torch.cuda.synchronize()
+        acc["runs"][st] = {"u": rel(ug[fl], uo[fl]), "rho": rel(rg[fl], ro[fl]),
+                           "mask_equal": bool(np.array_equal(cls_g, cls_o) and np.array_equal(links_g, links_o))}
+    return acc, base
+
+
+def same_precision(args, mask, stream):
+    """FP64 storage (the reference's precision) on the same lattice: MLUPS and roofline."""
+    from lbflow_b200 import _abi
+    from lbflow_b200.domain import Domain
+    p = params_for(argparse.Namespace(**{**vars(args), "storage": "f64"}), mask)
+    n_fluid = int(np.count_nonzero(mask == 0))
+    steps = max(20, min(args.steps, 200))
+    with Domain(p) as d:
+        configure(d, args, _abi)
+        d.init(stream)
+        ms = time_steps(d, steps, 3, stream, 1)
+        sweep = sweep_name(d, _abi)
+    per = ms / 1e3 / steps
+    alg = n_fluid * 2 * 19 * 8 + mask.size
+    peak, kind = peaks()
+    return {"storage": "f64", "value": n_fluid / per / 1e6, "unit": "MLUPS", "steps": steps,
+            "ms_per_step": 1e3 * per, "roofline_frac": alg / per / 1e9 / peak, "peak_source": kind,
+            "algorithmic_bytes_per_launch": alg, "sweep": sweep}
+
+
+def run_engine(args, rank, world, local_rank):
+    import torch
+    from lbflow_b200 import _abi
+    from lbflow_b200.domain import Domain
+
+    torch.cuda.set_device(local_rank)
+    mask = geometry(args.n, args.seed, args.porosity)
+    p = params_for(args, mask)
+    n_fluid = int(np.count_nonzero(mask == 0))
+    N = mask.size
+    stream = torch.cuda.current_stream()
+    tuned = None
+    if args.autotune:
+        from lbflow_b200 import autotune
+        tuned = autotune.autotune(p, steps=20, cache=None)
+    dom = Domain(p)
+    configure(dom, args, _abi, tuned)
+    dom.init(stream)
+    sweep = sweep_name(dom, _abi)
+    sweep_key = "sparse" if dom.get_option(_abi.LBF_OPT_SPARSE) else "dense"
+    if tuned is not None:
+        sweep += f" (autotuned: {tuned.get('sweep')}, block_x {tuned.get('block_x', 0)})"
+    # the clock sampler starts before the warm-up so that its samples cover the timed steps
+    with Clocks(local_rank) as clk:
+        ms = time_steps(dom, args.steps, args.warmup, stream, world)
     clocks = clk.summary()
+    dom.close()
     sec = ms / 1e3
     mlups = world * n_fluid * args.steps / sec / 1e6
     # roofline of the step kernel (one launch per step)
@@ -293,33 +430,15 @@ def run_engine(args, rank, world, local_rank):
     per_launch = sec / args.steps
     achieved = alg_bytes / per_launch / 1e9
     peak, peak_kind = peaks()
-    traffic = profile_traffic(args.storage, args.n)
-    # end to end through lbf_solve with host buffers
-    e2e = None
-    if not args.no_e2e:
-        del dom
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
-        wall0 = time.perf_counter()
-        solve_arrays(p, args.steps, stream=stream)
-        t1.record(stream)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - wall0
-        e_ms = t0.elapsed_time(t1)
-        e_sec = max(e_ms / 1e3, wall)
-        if world > 1:
-            t = torch.tensor([e_sec], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_sec = float(t.item())
-        e2e = {"value": world * n_fluid * args.steps / e_sec / 1e6, "unit": "MLUPS",
-               "h2d_bytes_per_step": N / args.steps, "d2h_bytes_per_step": N * 4 * 8 / args.steps,
-               "note": "lbf_solve: node-type upload, init, K steps, density+velocity download (FP64) per solve"}
+    traffic = traffic_of(sweep_key, args.storage, args.n)
+    e2e = None if args.no_e2e else measure_e2e(args, p, n_fluid, N, stream, world)
     if rank != 0:
         return
-    base = None if args.no_cpu_baseline else cpu_baseline(args, mask)
+    acc, base = (None, None)
+    if not args.no_cpu_baseline:
+        stores = [args.storage] + ([x for x in ("f32", "f16dev") if x != args.storage])
+        acc, base = accuracy_vs_oracle(args, mask, args.acc_steps or 100, stores)
+    same = None if args.storage == "f64" or args.no_same_precision else same_precision(args, mask, stream)
     line = {"metric": "MLUPS", "value": mlups, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.storage != "f64" else "f64",
@@ -328,6 +447,7 @@ def run_engine(args, rank, world, local_rank):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes},
+            "accuracy": acc, "same_precision": same,
             "cpu_baseline": base, "e2e": e2e, "gpu_launches": args.steps, "clocks": clocks}
     print(json.dumps(line), flush=True)
 
@@ -440,7 +560,7 @@ def run_slabs(args, rank, world, local_rank):
                        "halo_bytes_per_step_per_gpu": 2 * halo,
                        "l2": f"inputs larger than L2 (populations 2 x 19 x {s_b} B per fluid node and GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": profile_traffic(args.storage, args.n), "peak_source": peak_kind,
+                         "traffic": traffic_of("sparse", args.storage, args.n), "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "note": "per GPU, step kernels + halo exchange in the timed step; the exchange "
                                  "(pack, NCCL send/recv, unpack on a second stream) overlaps the interior sweep"},

@@ -52,7 +52,10 @@ enum { LBF_D2Q5 = 0, LBF_D2Q9 = 1, LBF_D3Q15 = 2, LBF_D3Q19 = 3, LBF_D3Q27 = 4 }
 enum { LBF_WEST = 0, LBF_EAST = 1, LBF_SOUTH = 2, LBF_NORTH = 3, LBF_BOTTOM = 4, LBF_TOP = 5 };
 
 /* CollisionOperator::{BGK(tau), TRT(omega_plus, omega_minus), MRT(rates)} (src/lib.rs:37-42). */
-enum { LBF_BGK = 0, LBF_TRT = 1, LBF_MRT = 2 };
+/* LBF_CENTRAL: central-moment collision of the tensor-product sets D2Q9 and D3Q27
+ * (no reference counterpart): shear rate 1/tau; relaxation[0] = bulk rate,
+ * relaxation[1..4] = rates of the third to sixth orders (values <= 0 mean 1). */
+enum { LBF_BGK = 0, LBF_TRT = 1, LBF_MRT = 2, LBF_CENTRAL = 3 };
 
 /* momentum::bc::BoundaryCondition (src/momentum/bc.rs:12-26). */
 enum {
@@ -96,7 +99,7 @@ enum { LBF_COMPAT_REFERENCE = 0, LBF_COMPAT_PHYSICS = 1 };
 #define LBF_CLASS_FACE_SHIFT  2      /* bit 2+f: fluid node on face f (lattice.rs:163-175)     */
 
 typedef struct {
-    int32_t kind;                 /* LBF_BGK / LBF_TRT / LBF_MRT                      */
+    int32_t kind;                 /* LBF_BGK / LBF_TRT / LBF_MRT / LBF_CENTRAL        */
     int32_t _pad;
     double tau;                   /* BGK(tau)                                         */
     double omega_plus;            /* TRT(omega_plus, omega_minus): relaxation rates   */
@@ -230,9 +233,23 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  *                  node); 0 = dense layout; default: sparse on the lean path when at
  *                  least 5 % of the nodes are solid.  Set before lbf_domain_init.
  *                  get: 1 when in effect.
+ * LBF_OPT_STREAMING  streaming scheme of the sparse layout on the lean path:
+ *                  LBF_STREAM_PULL (two buffers; each step reads its neighbours'
+ *                  slots), LBF_STREAM_PUSH (two buffers; each step reads its own slots
+ *                  and writes its neighbours'), LBF_STREAM_INPLACE (AA pattern: one
+ *                  buffer; an even step reads and writes each node's own slots, an
+ *                  odd step its neighbours').  All three compute the same values bit
+ *                  for bit; the in-place scheme needs half the population memory.
+ *                  Default (-1): LBF_STREAM_PUSH; z-slabs always pull, and so do
+ *                  domains with explicit faces or a scalar.  Set before
+ *                  lbf_domain_init.  get: the scheme in effect.
+ * LBF_OPT_SROUND   16-bit deviation storage: 1 = stochastic rounding of the stored
+ *                  values (seeded by node and time step, so runs repeat exactly),
+ *                  0 = round to nearest; default 1.
  * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
 enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4,
-       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6, LBF_OPT_SPARSE = 7 };
+       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6, LBF_OPT_SPARSE = 7, LBF_OPT_STREAMING = 8, LBF_OPT_SROUND = 9 };
+enum { LBF_STREAM_PULL = 0, LBF_STREAM_PUSH = 1, LBF_STREAM_INPLACE = 2 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);
 /* Number of main_steps executed so far (the reference's time_step). */
@@ -289,18 +306,18 @@ lbf_status lbf_domain_step_part(lbf_domain* dom, int32_t part, int64_t residual_
 
 /* ---- FP64 fluid sums with no device allocation --------------------------- */
 /* No counterpart in the reference (whose reductions are rayon sums on the CPU).
- * For callers that cannot allocate device memory when they need the sums: code
- * inside a CUDA stream capture, where allocation calls are not allowed, or hosts
- * whose HBM is already reserved by their own allocator or by lattices sized to
- * fill it.  Computes [sum rho, sum rho*u_a (d values), sum C, sum q_ads] over the
+ * For callers that cannot allocate device memory when they need the sums: hosts
+ * whose HBM is already reserved by their own caching allocator (an allocation
+ * behind its back breaks its accounting) or by lattices sized to fill it (an
+ * allocation would fail).  Computes [sum rho, sum rho*u_a (d values), sum C, sum q_ads] over the
  * nodes whose node_class lacks LBF_CLASS_SOLID, from caller-owned device arrays
  * (density[n], velocity[n*d], optional scalar[n] and q_ads[n], node_class[n] as
  * returned by lbf_domain_get_node_class), into the caller-owned device array
  * out[3 + d].  Scratch lives in a fixed 16 KiB static device array that every
  * GPU loading the library holds until exit; each call clears it first, and calls
  * that overlap on the GPU race on it.  The first call on a device looks up that
- * array's address (cudaGetSymbolAddress) with the device current: make it before
- * any stream capture.  Rejects n > LBF_NOALLOC_MAX_NODES and d outside {2, 3}. */
+ * array's address (cudaGetSymbolAddress) with the device current and loads the
+ * entry point's kernels: make it before any stream capture.  Rejects n > LBF_NOALLOC_MAX_NODES and d outside {2, 3}. */
 #define LBF_NOALLOC_MAX_NODES 2147483647LL
 lbf_status lbf_inventory_noalloc(const double* density, const double* velocity, const double* scalar,
                                  const double* q_ads, const uint32_t* node_class, int64_t n, int32_t d,

@@ -8,7 +8,7 @@ host side: the reference's parameter types (`momentum`, `passive_scalar`), the
 `solve` driver with the reference's file outputs, and ctypes bindings.
 """
 from . import _abi, core, io, momentum, passive_scalar  # noqa: F401
-from .core import (BGK, MRT, TRT, BoundaryFace, CollisionOperator, Compat, NodeType,  # noqa: F401
+from .core import (BGK, MRT, TRT, BoundaryFace, CentralMoment, CollisionOperator, Compat, NodeType,  # noqa: F401
                    Storage, VelocitySet)
 
 __all__ = ["momentum", "passive_scalar", "io", "core", "BGK", "TRT", "MRT", "BoundaryFace",

@@ -16,7 +16,7 @@ STATUS_NAMES = {0: "OK", 1: "EINVAL", 2: "ENOMEM", 3: "EDEVICE", 4: "ETIMEOUT", 
 
 LBF_D2Q5, LBF_D2Q9, LBF_D3Q15, LBF_D3Q19, LBF_D3Q27 = range(5)
 LBF_WEST, LBF_EAST, LBF_SOUTH, LBF_NORTH, LBF_BOTTOM, LBF_TOP = range(6)
-LBF_BGK, LBF_TRT, LBF_MRT = range(3)
+LBF_BGK, LBF_TRT, LBF_MRT, LBF_CENTRAL = range(4)
 LBF_BC_NO_SLIP, LBF_BC_BOUNCE_BACK, LBF_BC_ANTI_BOUNCE_BACK, LBF_BC_ZOU_HE, LBF_BC_PERIODIC = range(5)
 (LBF_SBC_ANTI_BOUNCE_BACK, LBF_SBC_ANTI_BB_NO_FLUX, LBF_SBC_BB_NO_FLUX,
  LBF_SBC_ZEROTH_ORDER_NO_FLUX, LBF_SBC_SECOND_ORDER_NO_FLUX, LBF_SBC_PERIODIC) = range(6)
@@ -25,7 +25,8 @@ LBF_STORE_F64, LBF_STORE_F32, LBF_STORE_F16DEV, LBF_STORE_BF16DEV = range(4)
 LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 
 (LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END,
- LBF_OPT_SPARSE) = range(8)
+ LBF_OPT_SPARSE, LBF_OPT_STREAMING, LBF_OPT_SROUND) = range(10)
+LBF_STREAM_PULL, LBF_STREAM_PUSH, LBF_STREAM_INPLACE = range(3)
 
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2

@@ -19,7 +19,7 @@ import numpy as np
 
 from . import momentum as m
 from . import passive_scalar as ps
-from .core import BGK, MRT, TRT, BoundaryFace, Compat, Storage, VelocitySet
+from .core import BGK, MRT, TRT, BoundaryFace, CentralMoment, Compat, Storage, VelocitySet
 
 W, E, S, N, B, T = (BoundaryFace.West, BoundaryFace.East, BoundaryFace.South, BoundaryFace.North,
                     BoundaryFace.Bottom, BoundaryFace.Top)
@@ -116,9 +116,11 @@ def tgv_rates(tau: float, q: int = 27, other: float = 1.0) -> list:
 
 
 def tgv_d3q27(n: int = 384, u0: float = 0.05, re: float = 1600.0, storage: Storage = Storage.F32,
-              other_rate: float = 1.0) -> Tuple[m.Parameters, float]:
+              other_rate: float = 1.0, collision: str = "mrt") -> Tuple[m.Parameters, float]:
     """Taylor-Green vortex: u = u0 (sin x cos y cos z, -cos x sin y cos z, 0), rho = 1,
-    x = 2 pi (i + 1/2) / n, nu = u0 (n / 2 pi) / Re; returns (params, nu)."""
+    x = 2 pi (i + 1/2) / n, nu = u0 (n / 2 pi) / Re; returns (params, nu).
+    collision: "mrt" (raw-moment MRT on the engine's D3Q27 basis) or "central"
+    (central moments, higher orders relaxed with `other_rate`)."""
     nu = u0 * (n / (2.0 * math.pi)) / re
     tau = 3.0 * nu + 0.5
     i = (np.arange(n) + 0.5) * 2.0 * math.pi / n
@@ -126,7 +128,9 @@ def tgv_d3q27(n: int = 384, u0: float = 0.05, re: float = 1600.0, storage: Stora
     u = np.zeros((n, n, n, 3))
     u[..., 0] = u0 * np.sin(x) * np.cos(y) * np.cos(z)
     u[..., 1] = -u0 * np.cos(x) * np.sin(y) * np.cos(z)
-    p = m.Parameters(n=[n, n, n], collision_operator=MRT(tgv_rates(tau, 27, other_rate)),
+    op = (CentralMoment(tau, other_rate, (other_rate,) * 4) if collision == "central"
+          else MRT(tgv_rates(tau, 27, other_rate)))
+    p = m.Parameters(n=[n, n, n], collision_operator=op,
                      velocity_set=VelocitySet.D3Q27, initial_density=m.InitialDensity.Uniform(1.0),
                      initial_velocity=m.InitialVelocity.FromArray(u.reshape(-1, 3)),
                      boundary_conditions=[(f, m.Periodic) for f in (W, E, S, N, B, T)], storage=storage)

@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import enum
 from dataclasses import dataclass, field
-from typing import List
+from typing import List, Tuple
 
 from . import _abi
 
@@ -113,9 +113,31 @@ class MRT(CollisionOperator):
         return d
 
 
+@dataclass(frozen=True)
+class CentralMoment(CollisionOperator):
+    """Central-moment collision of the tensor-product sets D2Q9 and D3Q27 (engine
+    extension; the reference has no D3Q27 collision): shear relaxation 1/tau,
+    the trace of the second-order moments at `bulk`, third to sixth orders at
+    `higher` (four rates; 1 relaxes them fully to the equilibrium)."""
+    tau: float
+    bulk: float = 1.0
+    higher: Tuple[float, float, float, float] = (1.0, 1.0, 1.0, 1.0)
+
+    def to_desc(self):
+        d = _abi.CollisionDesc()
+        d.kind = _abi.LBF_CENTRAL
+        d.tau = float(self.tau)
+        d.relaxation[0] = float(self.bulk)
+        for i, w in enumerate(self.higher):
+            d.relaxation[1 + i] = float(w)
+        return d
+
+
 def collision_from_desc(d: _abi.CollisionDesc, q: int) -> CollisionOperator:
     if d.kind == _abi.LBF_BGK:
         return BGK(d.tau)
     if d.kind == _abi.LBF_TRT:
         return TRT(d.omega_plus, d.omega_minus)
+    if d.kind == _abi.LBF_CENTRAL:
+        return CentralMoment(d.tau, d.relaxation[0], tuple(d.relaxation[1 + i] for i in range(4)))
     return MRT([d.relaxation[i] for i in range(q)])

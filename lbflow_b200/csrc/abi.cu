@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
@@ -129,6 +130,63 @@ void pinned64_free(void* p) {
     if (!p) return;
     std::lock_guard<std::mutex> lk(g_pin_mu);
     g_pin_free.push_back(p);
+}
+
+// Device -> host copies of large results into caller memory (pageable, as a
+// numpy array is): the bytes go through two pinned staging buffers, so the DMA
+// of one chunk overlaps the host threads' copy of the previous one out of
+// pinned memory.  The staging buffers are allocated once per process.
+constexpr size_t STAGE_CHUNK = 32u << 20;
+std::mutex g_stage_mu;
+char* g_stage[2] = {nullptr, nullptr};
+cudaEvent_t g_stage_ev[2] = {nullptr, nullptr};
+
+void host_copy_parallel(char* dst, const char* src, size_t bytes) {
+    const size_t per = 4u << 20;
+    const int nt = (int)std::min<size_t>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())),
+                                         (bytes + per - 1) / per);
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (bytes + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const size_t a = (size_t)t * part, b = std::min(bytes, a + part);
+        if (a < b) th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+    }
+    for (auto& x : th) x.join();
+}
+
+cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes < (4u << 20)) {
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
+    std::lock_guard<std::mutex> lk(g_stage_mu);
+    if (!g_stage[0]) {
+        for (int k = 0; k < 2; ++k) {
+            cudaError_t e = cudaMallocHost((void**)&g_stage[k], STAGE_CHUNK);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g_stage_ev[k], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    const size_t n = (bytes + STAGE_CHUNK - 1) / STAGE_CHUNK;
+    for (size_t c = 0; c <= n; ++c) {
+        if (c < n) {   // chunk c into buffer c & 1 (free: its previous chunk was copied out below)
+            const size_t off = c * STAGE_CHUNK, len = std::min(STAGE_CHUNK, bytes - off);
+            cudaError_t e = cudaMemcpyAsync(g_stage[c & 1], (const char*)src + off, len, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecord(g_stage_ev[c & 1], s);
+            if (e != cudaSuccess) return e;
+        }
+        if (c > 0) {   // chunk c - 1 is in flight or landed: copy it out while chunk c transfers
+            const size_t off = (c - 1) * STAGE_CHUNK, len = std::min(STAGE_CHUNK, bytes - off);
+            cudaError_t e = cudaEventSynchronize(g_stage_ev[(c - 1) & 1]);
+            if (e != cudaSuccess) return e;
+            host_copy_parallel((char*)dst + off, g_stage[(c - 1) & 1], len);
+        }
+    }
+    return cudaSuccess;
 }
 
 // ---- D3Q27 orthogonal moment basis (no reference counterpart: the reference's
@@ -261,6 +319,10 @@ struct lbf_domain {
     std::vector<long long> zoff;  // sparse: first fluid index of each z plane, then the fluid count
     int rw_w = 0;                 // sparse: words per row
     bool sparse_packed = false;   // sparse: list entries hold packed coordinates
+    int stream_opt = -1;          // LBF_OPT_STREAMING: streaming scheme of the lean sparse layout (-1 auto)
+    bool inplace = false;         // in effect: AA pattern, one population buffer (pop[0]); steps alternate even / odd
+    bool push = false;            // in effect: push sweep (two buffers, the state is the post-stream field)
+    int sround = 1;               // 16-bit storage: stochastic rounding
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
     long long nlist = 0;
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
@@ -486,14 +548,23 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     }
     dev_free(flag, D->dev); dev_free(val, D->dev); dev_free(nsel, D->dev); dev_free(tmp, D->dev);
     dev_free(bits, D->dev); dev_free(cnt, D->dev); dev_free(off, D->dev);
-    // population planes of fluid slots only
+    // population planes of fluid slots only (one buffer when streaming in place)
     const long long Fp = (F + 63) / 64 * 64;
     const size_t eb = st_bytes(D->st);
+    const bool lean = !D->facebc && !D->scalar;
+    const bool whole = !z_restricted(D) && lean;
+    const int scheme = D->stream_opt < 0 ? LBF_STREAM_PUSH : D->stream_opt;
+    const bool inplace = whole && scheme == LBF_STREAM_INPLACE;
+    D->push = whole && scheme == LBF_STREAM_PUSH;
     void* np[2] = {nullptr, nullptr};
+    void* ng[2] = {nullptr, nullptr};
+    const size_t rb = rt_bytes(D->st);
     if (e == cudaSuccess) e = dev_alloc(&np[0], (size_t)D->q * Fp * eb, D->dev);
-    if (e == cudaSuccess) e = dev_alloc(&np[1], (size_t)D->q * Fp * eb, D->dev);
+    if (e == cudaSuccess && !inplace) e = dev_alloc(&np[1], (size_t)D->q * Fp * eb, D->dev);
+    for (int k = 0; k < 2 && e == cudaSuccess && D->scalar; ++k) e = dev_alloc(&ng[k], (size_t)D->q * Fp * rb, D->dev);
     if (e != cudaSuccess) {
         dev_free(flist, D->dev); dev_free(np[0], D->dev); dev_free(np[1], D->dev);
+        dev_free(ng[0], D->dev); dev_free(ng[1], D->dev);
         dev_free(D->fmask, D->dev); dev_free(D->rw, D->dev);
         D->fmask = nullptr; D->rw = nullptr;
         cudaGetLastError();
@@ -505,8 +576,17 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     dev_free(D->pop[1], D->dev);
     D->pop[0] = np[0];
     D->pop[1] = np[1];
+    if (D->scalar) {
+        const long long old_g = 2ll * D->q * D->Np * (long long)rb;
+        dev_free(D->gpop[0], D->dev);
+        dev_free(D->gpop[1], D->dev);
+        D->gpop[0] = ng[0];
+        D->gpop[1] = ng[1];
+        D->bytes += 2ll * D->q * Fp * (long long)rb - old_g;
+    }
     D->Np = Fp;
-    D->bytes += 2ll * D->q * Fp * (long long)eb - old_bytes + F * 8 + (nw + W) * 8;
+    D->inplace = inplace;
+    D->bytes += (inplace ? 1ll : 2ll) * D->q * Fp * (long long)eb - old_bytes + F * 8 + (nw + W) * 8;
     D->list = flist;
     D->nlist = F;
     D->rw_w = W;
@@ -580,10 +660,11 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     }
     D->nlist = 0;
     if (D->list) { dev_free(D->list, D->dev); D->list = nullptr; }
-    // the sparse sweep also serves z-slabs (it updates the fluid slots of the owned planes)
+    // the sparse sweep also serves z-slabs (it updates the fluid slots of the owned
+    // planes) and, whole lattices only, explicit faces and the scalar
     const bool lean = !D->facebc && !D->scalar;
     const bool porous = (double)D->n_fluid <= 0.95 * (double)N;
-    if (lean && (D->sparse_opt > 0 || (D->sparse_opt < 0 && porous)) && !D->initialized) {
+    if ((lean || !z_restricted(D)) && (D->sparse_opt > 0 || (D->sparse_opt < 0 && porous)) && !D->initialized) {
         if ((st = build_sparse(D, s))) return st;
         if (D->sparse) {
             D->compact = false;
@@ -621,15 +702,24 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.np = D->Np;
     P.packed = D->sparse_packed ? 1 : 0;
     const size_t eb = st_bytes(D->st);
+    // in place: one buffer, read and written by every step (even and odd placements)
+    const int rd = D->inplace ? 0 : (int)(t & 1), wr = D->inplace ? 0 : (int)((t + 1) & 1);
     for (int i = 0; i < D->q; ++i) {
-        P.srcp[i] = (const char*)D->pop[t & 1] + (size_t)i * D->Np * eb;
-        P.dstp[i] = (char*)D->pop[(t + 1) & 1] + (size_t)i * D->Np * eb;
+        P.srcp[i] = (const char*)D->pop[rd] + (size_t)i * D->Np * eb;
+        P.dstp[i] = (char*)D->pop[wr] + (size_t)i * D->Np * eb;
     }
+    P.sweep_mode = D->inplace ? ((t & 1) ? SWEEP_AA_ODD : SWEEP_AA_EVEN) : (D->push ? SWEEP_PUSH : SWEEP_PULL);
+    P.sround = D->sround;
+    P.tstep = (unsigned)t;
     const lbf_collision_desc& c = D->desc.collision;
     P.coll = c.kind; P.compat = D->desc.compat; P.has_force = D->desc.has_force; P.first = t == 0;
-    P.tau = c.tau; P.omega = c.kind == LBF_BGK ? 1.0 / c.tau : 0.0; P.op = c.omega_plus; P.om = c.omega_minus;
+    P.tau = c.tau;
+    P.omega = (c.kind == LBF_BGK || c.kind == LBF_CENTRAL) ? 1.0 / c.tau : 0.0;
+    P.op = c.omega_plus; P.om = c.omega_minus;
     P.bgk_cb = c.kind == LBF_BGK ? 1.0 - 0.5 / c.tau : 0.0;
     for (int k = 0; k < 27; ++k) P.rates[k] = c.relaxation[k];
+    if (c.kind == LBF_CENTRAL)   // bulk, 3rd .. 6th order rates; <= 0 means full relaxation
+        for (int k = 0; k < 5; ++k) P.rates[k] = c.relaxation[k] > 0.0 ? c.relaxation[k] : 1.0;
     for (int a = 0; a < 3; ++a) P.force[a] = D->desc.has_force ? D->desc.force[a] : 0.0;
     fill_face_params(D, P);
     P.any_face = 0;
@@ -688,63 +778,79 @@ bool can_pipe(const lbf_domain* D) {
     return !D->facebc && !D->scalar && rowb % 16 == 0 && 2 * D->q * rowb <= 200 * 1024;
 }
 
+// Calls fn(IC<VS>, IC<COLL>) for the domain's velocity set and collision (the
+// central-moment collision exists for the tensor-product sets only).
+template <class Fn>
+cudaError_t by_kind(const lbf_domain* D, Fn&& fn) {
+    const int c = D->desc.collision.kind;
+    switch (D->vs) {
+        case LBF_D2Q9:
+            switch (c) {
+                case LBF_BGK: return fn(IC<VS_D2Q9>{}, IC<COLL_BGK>{});
+                case LBF_TRT: return fn(IC<VS_D2Q9>{}, IC<COLL_TRT>{});
+                case LBF_MRT: return fn(IC<VS_D2Q9>{}, IC<COLL_MRT>{});
+                default: return fn(IC<VS_D2Q9>{}, IC<COLL_CENTRAL>{});
+            }
+        case LBF_D3Q19:
+            switch (c) {
+                case LBF_BGK: return fn(IC<VS_D3Q19>{}, IC<COLL_BGK>{});
+                case LBF_TRT: return fn(IC<VS_D3Q19>{}, IC<COLL_TRT>{});
+                case LBF_MRT: return fn(IC<VS_D3Q19>{}, IC<COLL_MRT>{});
+                default: return cudaErrorInvalidValue;
+            }
+        default:
+            switch (c) {
+                case LBF_BGK: return fn(IC<VS_D3Q27>{}, IC<COLL_BGK>{});
+                case LBF_TRT: return fn(IC<VS_D3Q27>{}, IC<COLL_TRT>{});
+                case LBF_MRT: return fn(IC<VS_D3Q27>{}, IC<COLL_MRT>{});
+                default: return fn(IC<VS_D3Q27>{}, IC<COLL_CENTRAL>{});
+            }
+    }
+}
+const double* lam_of(const lbf_domain* D) { return D->lam.empty() ? nullptr : D->lam.data(); }
+
 cudaError_t launch_pipe(lbf_domain* D, const StepParams& P, cudaStream_t s) {
     const size_t stage_b = (size_t)D->q * D->n[0] * st_bytes(D->st);
     // three blocks of <= 288 threads per SM share ~220 KB of shared memory
     int stages = D->pipe_stages > 0 ? D->pipe_stages : (int)std::max<size_t>(2, std::min<size_t>(8, (72 * 1024) / stage_b));
     while (stages > 2 && stages * stage_b > 200 * 1024) --stages;
     const int nc = (int)std::min<long long>(8, std::max<long long>(1, (D->n[0] + 31) / 32));
-    const int coll = D->desc.collision.kind;
-    switch (D->vs) {
-        case LBF_D2Q9:
-            return coll == LBF_BGK ? launch_step_pipe<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, stages, nc, s)
-                 : coll == LBF_TRT ? launch_step_pipe<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, stages, nc, s)
-                                   : launch_step_pipe<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, stages, nc, s);
-        case LBF_D3Q19:
-            return coll == LBF_BGK ? launch_step_pipe<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, stages, nc, s)
-                 : coll == LBF_TRT ? launch_step_pipe<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, stages, nc, s)
-                                   : launch_step_pipe<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, stages, nc, s);
-        default:
-            return coll == LBF_BGK ? launch_step_pipe<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), stages, nc, s)
-                 : coll == LBF_TRT ? launch_step_pipe<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), stages, nc, s)
-                                   : launch_step_pipe<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), stages, nc, s);
-    }
+    return by_kind(D, [&](auto V, auto C) {
+        return launch_step_pipe<decltype(V)::value, decltype(C)::value>(D->st, P, lam_of(D), stages, nc, s);
+    });
 }
 
 cudaError_t launch_list(lbf_domain* D, const StepParams& P, cudaStream_t s) {
-    const int coll = D->desc.collision.kind;
-    switch (D->vs) {
-        case LBF_D2Q9:
-            return coll == LBF_BGK ? launch_step_list<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, s)
-                 : coll == LBF_TRT ? launch_step_list<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, s)
-                                   : launch_step_list<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, s);
-        case LBF_D3Q19:
-            return coll == LBF_BGK ? launch_step_list<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, s)
-                 : coll == LBF_TRT ? launch_step_list<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, s)
-                                   : launch_step_list<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, s);
-        default:
-            return coll == LBF_BGK ? launch_step_list<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), s)
-                 : coll == LBF_TRT ? launch_step_list<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), s)
-                                   : launch_step_list<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), s);
+    return by_kind(D, [&](auto V, auto C) {
+        return launch_step_list<decltype(V)::value, decltype(C)::value>(D->st, P, lam_of(D), s);
+    });
+}
+
+// Sparse sweep with explicit faces and/or the scalar: the bulk launch, then one
+// face pass per scalar outflow face (as launch_step_any does for the dense sweep).
+cudaError_t launch_sparse_fs(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    auto one = [&](const StepParams& Q, unsigned blocks) -> cudaError_t {
+        return by_kind(D, [&](auto V, auto C) {
+            return launch_step_sparse_fs<decltype(V)::value, decltype(C)::value>(D->st, D->scalar, Q, lam_of(D),
+                                                                                 blocks, s);
+        });
+    };
+    cudaError_t e = one(P, (unsigned)((P.kend - P.kbeg + 255) / 256));
+    for (int f = 0; f < D->nfaces && e == cudaSuccess; ++f) {
+        if (!(D->outflow >> f & 1u)) continue;
+        StepParams F = P;
+        F.face_pass = 1;
+        F.fp_face = f;
+        e = one(F, (unsigned)((D->pb_plane[f] + 255) / 256));
     }
+    return e;
 }
 
 cudaError_t launch_sparse(lbf_domain* D, const StepParams& P, cudaStream_t s) {
-    const int coll = D->desc.collision.kind;
-    switch (D->vs) {
-        case LBF_D2Q9:
-            return coll == LBF_BGK ? launch_step_sparse<VS_D2Q9, COLL_BGK>(D->st, P, nullptr, s)
-                 : coll == LBF_TRT ? launch_step_sparse<VS_D2Q9, COLL_TRT>(D->st, P, nullptr, s)
-                                   : launch_step_sparse<VS_D2Q9, COLL_MRT>(D->st, P, nullptr, s);
-        case LBF_D3Q19:
-            return coll == LBF_BGK ? launch_step_sparse<VS_D3Q19, COLL_BGK>(D->st, P, nullptr, s)
-                 : coll == LBF_TRT ? launch_step_sparse<VS_D3Q19, COLL_TRT>(D->st, P, nullptr, s)
-                                   : launch_step_sparse<VS_D3Q19, COLL_MRT>(D->st, P, nullptr, s);
-        default:
-            return coll == LBF_BGK ? launch_step_sparse<VS_D3Q27, COLL_BGK>(D->st, P, D->lam.data(), s)
-                 : coll == LBF_TRT ? launch_step_sparse<VS_D3Q27, COLL_TRT>(D->st, P, D->lam.data(), s)
-                                   : launch_step_sparse<VS_D3Q27, COLL_MRT>(D->st, P, D->lam.data(), s);
-    }
+    if (D->facebc || D->scalar) return launch_sparse_fs(D, P, s);
+    return by_kind(D, [&](auto V, auto C) {
+        return launch_step_sparse<decltype(V)::value, decltype(C)::value>(D->st, P, lam_of(D), s);
+    });
 }
 
 // The bulk sweep, then one face pass per scalar outflow face.
@@ -815,12 +921,21 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     void* pb[12];
     for (int f = 0; f < 6; ++f) { pb[2 * f] = D->pb[f][0]; pb[2 * f + 1] = D->pb[f][1]; }
     Launch L{dim3((unsigned)((D->N + 255) / 256)), dim3(256), s};
-    cudaError_t e;
-    if (D->sparse)
+    cudaError_t e = cudaSuccess;
+    if (D->sparse && (D->facebc || D->scalar)) {
+        // the per-node side arrays (residual moments, adsorbed amount, previous
+        // scalar value, face layers) by node; the populations by fluid slot below
+        I.skip_pops = 1;
+        e = D->vs == LBF_D2Q9 ? launch_init<VS_D2Q9>(D->st, D->scalar, P, I, pb, L)
+          : D->vs == LBF_D3Q19 ? launch_init<VS_D3Q19>(D->st, D->scalar, P, I, pb, L)
+                               : launch_init<VS_D3Q27>(D->st, D->scalar, P, I, pb, L);
+        I.skip_pops = 0;
+    }
+    if (e == cudaSuccess && D->sparse)
         e = D->vs == LBF_D2Q9 ? launch_init_sparse<VS_D2Q9>(D->st, P, I, s)
           : D->vs == LBF_D3Q19 ? launch_init_sparse<VS_D3Q19>(D->st, P, I, s)
                                : launch_init_sparse<VS_D3Q27>(D->st, P, I, s);
-    else
+    else if (e == cudaSuccess)
         e = D->vs == LBF_D2Q9 ? launch_init<VS_D2Q9>(D->st, D->scalar, P, I, pb, L)
           : D->vs == LBF_D3Q19 ? launch_init<VS_D3Q19>(D->st, D->scalar, P, I, pb, L)
                                : launch_init<VS_D3Q27>(D->st, D->scalar, P, I, pb, L);
@@ -908,6 +1023,7 @@ lbf_status halo_copy(lbf_domain* D, int face, bool unpack, void* buf, cudaStream
     if (face != LBF_BOTTOM && face != LBF_TOP) return fail(LBF_EINVAL, "halo face must be LBF_BOTTOM or LBF_TOP");
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
     if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
+    if (D->inplace || D->push) return fail(LBF_EUNSUPPORTED, "halos need the pull sweep (LBF_STREAM_PULL)");
     const long long z0 = zb(D), z1 = ze(D);
     if (z0 < 1 || z1 > D->n[2] - 1) return fail(LBF_EINVAL, "halos need a ghost plane below z_begin and above z_end - 1");
     // bottom: pack plane z0, c_z = -1; unpack ghost z0 - 1, c_z = +1
@@ -968,11 +1084,12 @@ struct Section {
     size_t bytes;
 };
 
-std::vector<Section> ckpt_sections(const lbf_domain* D) {
+// `t` selects the population buffers: the ones the step at time t reads.
+std::vector<Section> ckpt_sections(const lbf_domain* D, long long t) {
     std::vector<Section> s;
     const size_t eb = st_bytes(D->st), rb = rt_bytes(D->st);
-    s.push_back({D->pop[D->t & 1], (size_t)D->q * D->Np * eb});
-    s.push_back({D->scalar ? D->gpop[D->t & 1] : nullptr, D->scalar ? (size_t)D->q * D->Np * rb : 0});
+    s.push_back({D->pop[D->inplace ? 0 : (t & 1)], (size_t)D->q * D->Np * eb});
+    s.push_back({D->scalar ? D->gpop[t & 1] : nullptr, D->scalar ? (size_t)D->q * D->Np * rb : 0});
     s.push_back({D->qads, D->qads ? (size_t)D->N * rb : 0});
     s.push_back({D->cprev, D->cprev ? (size_t)D->N * rb : 0});
     for (int k = 0; k < 2; ++k)
@@ -1031,7 +1148,10 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     if (N >= (1ll << 31)) return fail(LBF_EINVAL, "more than 2^31 nodes");
     const lbf_collision_desc& c = ds->collision;
     if (c.kind == LBF_BGK && !(c.tau > 0.0)) return fail(LBF_EINVAL, "BGK tau must be > 0");
-    if (c.kind < LBF_BGK || c.kind > LBF_MRT) return fail(LBF_EINVAL, "bad collision kind");
+    if (c.kind < LBF_BGK || c.kind > LBF_CENTRAL) return fail(LBF_EINVAL, "bad collision kind");
+    if (c.kind == LBF_CENTRAL && !(c.tau > 0.0)) return fail(LBF_EINVAL, "central-moment tau must be > 0");
+    if (c.kind == LBF_CENTRAL && vs == LBF_D3Q19)
+        return fail(LBF_EUNSUPPORTED, "the central-moment collision needs a tensor-product set (D2Q9, D3Q27)");
     const int nf = d == 2 ? 4 : 6;
     for (int f = 0; f < nf; ++f) {
         std::string why;
@@ -1057,7 +1177,11 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     for (int a = 0; a < 3; ++a) D->n[a] = n[a];
     D->N = N;
     D->type.assign(N, 0);
-    if (ds->node_type) for (long long i = 0; i < N; ++i) D->type[i] = ds->node_type[i] ? 1 : 0;
+    if (ds->node_type) {
+        std::memcpy(D->type.data(), ds->node_type, (size_t)N);
+        // any non-zero value means solid: normalised to 1 (a no-op for 0 / 1 masks)
+        for (long long i = 0; i < N; ++i) D->type[i] = D->type[i] != 0;
+    }
     D->rho0u = ds->initial_density;
     for (int a = 0; a < 3; ++a) D->u0u[a] = ds->initial_velocity[a];
     if (ds->initial_density_field) D->rho0.assign(ds->initial_density_field, ds->initial_density_field + N);
@@ -1230,12 +1354,21 @@ lbf_status lbf_domain_get_moments(lbf_domain* D, double* rho, double* u, double*
     lbf_status st;
     if ((st = do_observe(D, s))) return st;
     const long long N = D->N;
-    if (rho) CK(cudaMemcpyAsync(rho, D->obs, N * 8, cudaMemcpyDeviceToHost, s));
-    if (u) CK(cudaMemcpyAsync(u, D->obs + N, N * D->d * 8, cudaMemcpyDeviceToHost, s));
-    if (c && D->scalar) CK(cudaMemcpyAsync(c, D->obs + N * (1 + D->d), N * 8, cudaMemcpyDeviceToHost, s));
+    // solid nodes keep their initial values (they are never updated): filled on the
+    // device when those are uniform
+    const bool uniform = D->rho0.empty() && D->u0.empty() && (!D->scalar || D->c0.empty());
+    if (uniform && D->n_fluid < (unsigned long long)N) {
+        k_fill_solid<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
+            D->dtype, N, D->d, D->obs, D->obs + N, D->scalar ? D->obs + N * (1 + D->d) : nullptr, D->rho0u,
+            D->u0u[0], D->u0u[1], D->u0u[2], D->scalar ? D->sdesc.initial_scalar_value : 0.0);
+        CK(cudaGetLastError());
+    }
+    if (rho) CK(download(rho, D->obs, N * 8, s));
+    if (u) CK(download(u, D->obs + N, N * D->d * 8, s));
+    if (c && D->scalar) CK(download(c, D->obs + N * (1 + D->d), N * 8, s));
     CK(cudaStreamSynchronize(s));
     if ((st = check_err(D))) return st;
-    // solid nodes keep their initial values (they are never updated)
+    if (uniform) return LBF_OK;
     for (long long i = 0; i < N; ++i) {
         if (!D->type[i]) continue;
         if (rho) rho[i] = D->rho0.empty() ? D->rho0u : D->rho0[i];
@@ -1338,6 +1471,14 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
             if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_SPARSE before lbf_domain_init");
             D->sparse_opt = value != 0 ? 1 : 0;
             return LBF_OK;
+        case LBF_OPT_STREAMING:
+            if (D->prepared) return fail(LBF_ESTATE, "set LBF_OPT_STREAMING before lbf_domain_init");
+            if (value < -1 || value > LBF_STREAM_INPLACE) return fail(LBF_EINVAL, "streaming: -1, PULL, PUSH or INPLACE");
+            D->stream_opt = (int)value;
+            return LBF_OK;
+        case LBF_OPT_SROUND:
+            D->sround = value != 0 ? 1 : 0;
+            return LBF_OK;
         case LBF_OPT_Z_BEGIN:
         case LBF_OPT_Z_END:
             if (D->prepared) return fail(LBF_ESTATE, "set the swept z planes before lbf_domain_init");
@@ -1360,6 +1501,10 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
         case LBF_OPT_PIPE_STAGES: *value = D->pipe_stages; return LBF_OK;
         case LBF_OPT_COMPACT: *value = (D->compact && D->list) ? 1 : 0; return LBF_OK;
         case LBF_OPT_SPARSE: *value = D->sparse ? 1 : 0; return LBF_OK;
+        case LBF_OPT_STREAMING:
+            *value = D->inplace ? LBF_STREAM_INPLACE : (D->push ? LBF_STREAM_PUSH : LBF_STREAM_PULL);
+            return LBF_OK;
+        case LBF_OPT_SROUND: *value = D->sround; return LBF_OK;
         case LBF_OPT_Z_BEGIN: *value = zb(D); return LBF_OK;
         case LBF_OPT_Z_END: *value = ze(D); return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
@@ -1380,7 +1525,7 @@ lbf_status lbf_domain_checkpoint_bytes(lbf_domain* D, int64_t* bytes) {
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
     if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch");
     int64_t b = sizeof(CkptHeader);
-    for (const Section& s : ckpt_sections(D)) b += (int64_t)s.bytes;
+    for (const Section& s : ckpt_sections(D, D->t)) b += (int64_t)s.bytes;
     *bytes = b;
     return LBF_OK;
 }
@@ -1393,7 +1538,7 @@ lbf_status lbf_domain_save(lbf_domain* D, void* host, int64_t cap, void* stream)
     if (!host || cap < need) return fail(LBF_EINVAL, "checkpoint buffer smaller than lbf_domain_checkpoint_bytes");
     cudaStream_t s = (cudaStream_t)stream;
     CK(cudaStreamSynchronize(D->last_stream));
-    const std::vector<Section> secs = ckpt_sections(D);
+    const std::vector<Section> secs = ckpt_sections(D, D->t);
     CkptHeader h;
     std::memset(&h, 0, sizeof(h));
     std::memcpy(h.magic, "LBFCKPT1", 8);
@@ -1428,26 +1573,35 @@ lbf_status lbf_domain_load(lbf_domain* D, const void* host, int64_t bytes, void*
         h.sparse != (D->sparse ? 1 : 0) || (h.sparse && h.nlist != D->nlist) || h.scalar != (D->scalar ? 1 : 0) ||
         h.ads != (D->qads ? 1 : 0))
         return fail(LBF_EINVAL, "checkpoint of a different lattice, storage, layout or scalar set-up");
-    lbf_status st;
-    if ((h.sec_bytes[4] || h.sec_bytes[5]) && (st = ensure_mom(D))) return st;
-    cudaStream_t s = (cudaStream_t)stream;
-    CK(cudaStreamSynchronize(D->last_stream));
-    D->t = h.t;   // the sections of the state buffers follow the checkpoint's parity
-    const std::vector<Section> secs = ckpt_sections(D);
+    if (h.t < 0 || h.res_step < -1 || h.res_step > h.t) return fail(LBF_EINVAL, "checkpoint time step out of range");
+    // everything is validated before the domain changes: a rejected checkpoint
+    // leaves the time step, the residuals and every field as they were
+    const bool need_mom = h.sec_bytes[4] != 0 || h.sec_bytes[5] != 0;
+    std::vector<Section> secs = ckpt_sections(D, h.t);   // the buffers of the checkpoint's parity
     if (h.nsec != (int32_t)secs.size()) return fail(LBF_EINVAL, "checkpoint section count differs");
     int64_t total = sizeof(CkptHeader);
     for (size_t i = 0; i < secs.size(); ++i) {
-        if (h.sec_bytes[i] != (int64_t)secs[i].bytes && h.sec_bytes[i] != 0)
-            return fail(LBF_EINVAL, "checkpoint section sizes differ");
+        // the residual-moment buffers (sections 4, 5) are allocated on demand below
+        const int64_t want = (i == 4 || i == 5) && !secs[i].dev
+                                 ? (int64_t)D->nfields() * D->N * (int64_t)rt_bytes(D->st)
+                                 : (int64_t)secs[i].bytes;
+        if (h.sec_bytes[i] != want && h.sec_bytes[i] != 0) return fail(LBF_EINVAL, "checkpoint section sizes differ");
+        if (h.sec_bytes[i] < 0) return fail(LBF_EINVAL, "checkpoint section sizes differ");
         total += h.sec_bytes[i];
     }
     if (bytes < total) return fail(LBF_EINVAL, "checkpoint truncated");
+    lbf_status st;
+    if (need_mom && (st = ensure_mom(D))) return st;
+    secs = ckpt_sections(D, h.t);
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaStreamSynchronize(D->last_stream));
     const char* p = (const char*)host + sizeof(CkptHeader);
     for (size_t i = 0; i < secs.size(); ++i) {
         if (h.sec_bytes[i]) CK(cudaMemcpyAsync(secs[i].dev, p, (size_t)h.sec_bytes[i], cudaMemcpyHostToDevice, s));
         p += h.sec_bytes[i];
     }
     CK(cudaStreamSynchronize(s));
+    D->t = h.t;
     D->res_step = h.res_step;
     for (int i = 0; i < 8; ++i) D->res_host[i] = h.res[i];
     D->last_stream = s;
@@ -1698,7 +1852,7 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         // a large member runs its own sweep in the graph; its launch parameters are
         // fixed per chunk step only when k is even (t0 keeps its parity)
         const long long units = D->sparse ? D->nlist : D->N;
-        const bool solo = b->k % 2 == 0 && units >= SOLO_UNITS && !D->pipe && !D->stage;
+        const bool solo = b->k % 2 == 0 && (units >= SOLO_UNITS || (D->sparse && D->facebc)) && !D->pipe && !D->stage;
         lbf_batch::Group* g = nullptr;
         for (auto& x : b->groups)
             if (!solo && !x.solo && x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc &&
@@ -1880,6 +2034,11 @@ lbf_status lbf_batch_admit(lbf_batch* b, lbf_domain* D, int64_t max_iterations, 
     if (D->batch) return fail(LBF_ESTATE, "the domain is already in a batch");
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before lbf_batch_admit");
     if (D->scalar) return fail(LBF_EUNSUPPORTED, "domains with a scalar are not batched");
+    if (D->desc.collision.kind == LBF_CENTRAL)
+        return fail(LBF_EUNSUPPORTED, "domains with the central-moment collision are not batched");
+    if (D->sparse && D->facebc && b->k % 2)
+        return fail(LBF_EUNSUPPORTED, "a sparse-layout domain with explicit faces is batched with an even residual "
+                                      "interval only (it runs its own sweep in the chunk graph)");
     if (z_restricted(D)) return fail(LBF_EUNSUPPORTED, "z-slab domains are not batched");
     if (max_iterations < 0) return fail(LBF_EINVAL, "max_iterations must be >= 0");
     lbf_status st;

@@ -77,6 +77,8 @@ struct InitParams {
     const double* rho_field;   // or null
     const double* u_field;     // [N][D] or null
     const double* c_field;     // or null
+    int skip_pops;             // k_init: leave the populations (the sparse layout sets them by fluid slot)
+    int pad;
 };
 
 // Lattice::initialize_nodes (src/momentum/lattice.rs:322-328,
@@ -100,6 +102,7 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
     g.y = (int)((cell / P.nx) % P.ny);
     g.z = (int)(cell / ((long long)P.nx * P.ny));
     g.cell = cell;
+    g.slot = cell;
     const double rho = I0.rho_field ? I0.rho_field[cell] : I0.rho0;
     double u[3] = {I0.u0[0], I0.u0[1], I0.u0[2]};
     if (I0.u_field)
@@ -109,7 +112,7 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
     const bool fluid = !(mk & M_SOLID);
     double uu = 0.0;
     for (int a = 0; a < D; ++a) uu += u[a] * u[a];
-    if (fluid) {
+    if (fluid && !I0.skip_pops) {
         sfor<Q>([&](auto Ii) {
             constexpr int i = Ii;
             // FP32-compute formats store h = f_eq - w (evaluated in FP64)
@@ -176,6 +179,13 @@ __global__ void k_init_sparse(const StepParams P, const InitParams I0) {
         const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
         S::st(const_cast<void*>(P.srcp[i]), (int)k, S::sc(R(fe)));
     });
+    if (P.has_scalar) {   // g = g_eq(C0, u0) at the same slot (FP64 / FP32 storage only)
+        const double c0 = I0.c_field ? I0.c_field[cell] : I0.c0;
+        sfor<Q>([&](auto Ii) {
+            constexpr int i = Ii;
+            ((R*)P.gsrcp[i])[k] = R(feq_i<L, double>(i, c0, u, uu));
+        });
+    }
     if (P.mom_prev) {
         R* mp = (R*)P.mom_prev;
         mp[cell] = R(rho);
@@ -225,6 +235,19 @@ static __global__ void k_pack_xyz(uint32_t* list, long long n, int nx, int ny) {
     const uint32_t x = c % (uint32_t)nx, r = c / (uint32_t)nx;
     const uint32_t y = r % (uint32_t)ny, z = r / (uint32_t)ny;
     list[k] = x | (y << 11) | (z << 22);
+}
+
+// Solid nodes are never updated: their observed moments are the uniform initial
+// values (the observe pass writes the fluid nodes only).
+static __global__ void k_fill_solid(const uint8_t* type, long long N, int d, double* rho, double* u, double* c,
+                                    double rho0, double u0x, double u0y, double u0z, double c0) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= N || !type[i]) return;
+    rho[i] = rho0;
+    u[i * d] = u0x;
+    u[i * d + 1] = u0y;
+    if (d == 3) u[i * d + 2] = u0z;
+    if (c) c[i] = c0;
 }
 
 // Sum the NSLOT partials of each accumulator; out[k] = sqrt(sum) for residuals

@@ -45,6 +45,9 @@ __device__ __forceinline__ void batch_params(KParams<VS>& Ps, const KParams<VS>*
             Ps.mom_cur = const_cast<void*>(m);
         }
         Ps.first = t == 0;
+        if (Ps.sweep_mode == SWEEP_AA_EVEN || Ps.sweep_mode == SWEEP_AA_ODD)
+            Ps.sweep_mode = (t & 1) ? SWEEP_AA_ODD : SWEEP_AA_EVEN;
+        Ps.tstep = (unsigned)t;
         Ps.residual = k > 0 && t % k == 0;
         Ps.write_mom = k > 0 && (t % k == 0 || (t + 1) % k == 0);
     }
@@ -71,6 +74,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
     const bool inside = c64 < P.N;
     Geo g;
     g.cell = inside ? (int)c64 : 0;
+    g.slot = g.cell;
     {
         // coordinates by a double-precision reciprocal plus a +-1 correction
         auto divq = [](int n, int d, double inv) {
@@ -138,7 +142,12 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
     if (bs[e].done_t >= 0 || t > bs[e].last_t) return;   // uniform over the block
     batch_params<VS, COLL>(Ps, tab, e, t, bs[e].k);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    sparse_node<VS, COLL, ST>(Ps, (long long)(blockIdx.x - bs[e].block0) * BATCH_BLOCK + threadIdx.x, racc);
+    const long long k = (long long)(blockIdx.x - bs[e].block0) * BATCH_BLOCK + threadIdx.x;
+    // the sweep mode is uniform over the block (one domain per block)
+    if (Ps.sweep_mode == SWEEP_AA_EVEN) sparse_node<VS, COLL, ST, SWEEP_AA_EVEN>(Ps, k, racc);
+    else if (Ps.sweep_mode == SWEEP_AA_ODD) sparse_node<VS, COLL, ST, SWEEP_AA_ODD>(Ps, k, racc);
+    else if (Ps.sweep_mode == SWEEP_PUSH) sparse_node<VS, COLL, ST, SWEEP_PUSH>(Ps, k, racc);
+    else sparse_node<VS, COLL, ST, SWEEP_PULL>(Ps, k, racc);
     if (Ps.residual) block_accumulate<5>(racc, Ps.accum);
 }
 

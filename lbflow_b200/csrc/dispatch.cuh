@@ -115,12 +115,29 @@ cudaError_t launch_sparse_st(KParams<VS>& kp, cudaStream_t stream) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    kp.pf_blocks = sms * 2 * light_kernel<VS, COLL, ST, false>();
-    k_step_sparse<VS, COLL, ST><<<blocks, 256, 0, stream>>>(kp);
+    kp.pf_blocks = sms * (kp.sweep_mode == SWEEP_AA_ODD ? sparse_blocks<VS, COLL, ST, SWEEP_AA_ODD>()
+                                                        : sparse_blocks<VS, COLL, ST, SWEEP_PULL>());
+    switch (kp.sweep_mode) {
+        case SWEEP_AA_EVEN: k_step_sparse<VS, COLL, ST, SWEEP_AA_EVEN><<<blocks, 256, 0, stream>>>(kp); break;
+        case SWEEP_AA_ODD: k_step_sparse<VS, COLL, ST, SWEEP_AA_ODD><<<blocks, 256, 0, stream>>>(kp); break;
+        case SWEEP_PUSH: k_step_sparse<VS, COLL, ST, SWEEP_PUSH><<<blocks, 256, 0, stream>>>(kp); break;
+        default: k_step_sparse<VS, COLL, ST, SWEEP_PULL><<<blocks, 256, 0, stream>>>(kp); break;
+    }
     return cudaGetLastError();
 }
 template <int VS>
 cudaError_t launch_init_sparse(int st, const StepParams& P, const InitParams& I, cudaStream_t s);
+
+// Sparse sweep with explicit faces and/or a scalar (two buffers); the bulk
+// launch covers the fluid slots [kbeg, kend), a face pass the positions of a face.
+template <int VS, int COLL>
+cudaError_t launch_step_sparse_fs(int st, bool scalar, const StepParams& base, const double* lam, unsigned blocks,
+                                  cudaStream_t stream);
+#define LBF_SPARSE_FS_CASE(V_, C_, S_, SC_)                                                    \
+    if (st == S_ && scalar == SC_) {                                                           \
+        k_step_sparse_fs<V_, C_, S_, true, SC_><<<blocks, 256, 0, stream>>>(kp);                \
+        return cudaGetLastError();                                                             \
+    }
 
 // One translation unit per (velocity set, collision) instantiates the step kernels.
 template <int VS, int COLL>
@@ -184,7 +201,25 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
         }                                                                                              \
     }
 
-#define LBF_INSTANTIATE(VS_)                                                                           \
+#define LBF_INSTANTIATE_SPARSE_FS(VS_, COLL_)                                                          \
+    template <>                                                                                        \
+    cudaError_t launch_step_sparse_fs<VS_, COLL_>(int st, bool scalar, const StepParams& base,         \
+                                                  const double* lam, unsigned blocks, cudaStream_t stream) { \
+        if (blocks == 0) return cudaSuccess;                                                           \
+        KParams<VS_> kp;                                                                               \
+        static_cast<StepParams&>(kp) = base;                                                           \
+        fill_lam(kp, lam);                                                                             \
+        LBF_SPARSE_FS_CASE(VS_, COLL_, ST_F64, false) LBF_SPARSE_FS_CASE(VS_, COLL_, ST_F32, false)    \
+        LBF_SPARSE_FS_CASE(VS_, COLL_, ST_F16, false) LBF_SPARSE_FS_CASE(VS_, COLL_, ST_BF16, false)   \
+        LBF_SPARSE_FS_CASE(VS_, COLL_, ST_F64, true) LBF_SPARSE_FS_CASE(VS_, COLL_, ST_F32, true)      \
+        return cudaErrorInvalidValue;                                                                  \
+    }
+
+// The central-moment collision exists for the tensor-product sets only.
+#define LBF_CENTRAL_CASE_1(VS_) \
+    case COLL_CENTRAL: return launch_step_c<VS_, COLL_CENTRAL>(st, facebc, scalar, stage, base, lam, L);
+#define LBF_CENTRAL_CASE_0(VS_)
+#define LBF_INSTANTIATE(VS_, CENTRAL_)                                                                 \
     template <>                                                                                        \
     cudaError_t launch_step<VS_>(int coll, int st, bool facebc, bool scalar, bool stage,               \
                                  const StepParams& base, const double* lam, const Launch& L) {         \
@@ -192,6 +227,7 @@ cudaError_t launch_step_c(int st, bool facebc, bool scalar, bool stage, const St
             case COLL_BGK: return launch_step_c<VS_, COLL_BGK>(st, facebc, scalar, stage, base, lam, L); \
             case COLL_TRT: return launch_step_c<VS_, COLL_TRT>(st, facebc, scalar, stage, base, lam, L); \
             case COLL_MRT: return launch_step_c<VS_, COLL_MRT>(st, facebc, scalar, stage, base, lam, L); \
+            LBF_CENTRAL_CASE_##CENTRAL_(VS_)                                                           \
             default: return cudaErrorInvalidValue;                                                     \
         }                                                                                              \
     }                                                                                                  \

@@ -31,7 +31,7 @@
 
 namespace lbf {
 
-constexpr int COLL_BGK = 0, COLL_TRT = 1, COLL_MRT = 2;
+constexpr int COLL_BGK = 0, COLL_TRT = 1, COLL_MRT = 2, COLL_CENTRAL = 3;
 constexpr int ST_F64 = 0, ST_F32 = 1, ST_F16 = 2, ST_BF16 = 3;
 constexpr int COMPAT_REFERENCE = 0, COMPAT_PHYSICS = 1;
 
@@ -110,6 +110,10 @@ struct StepParams {
     const GateView* gate;     // batch member state, or null outside batches
     int gate_j;               // chunk step of this launch
     int packed;               // sparse list entries are x | y << 11 | z << 22 (else node indices)
+    int sweep_mode;           // sparse layout: SWEEP_PULL / SWEEP_PUSH (A/B buffers), SWEEP_AA_EVEN / _ODD (in place)
+    int sround;               // 16-bit storage: 1 = stochastic rounding (seeded by node and time step), 0 = nearest
+    unsigned tstep;           // time step of the launch (low 32 bits; the rounding seed)
+    int tpad;
     double bgk_cb, s_bgk_cb;  // 1 - 1/(2 tau) of the momentum and scalar BGK sources, computed once
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
@@ -167,6 +171,7 @@ struct Store<ST_F64> {
     __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
+    __device__ static __forceinline__ T enc(R v) { return v; }
 };
 template <>
 struct Store<ST_F32> {
@@ -178,6 +183,7 @@ struct Store<ST_F32> {
     __device__ static __forceinline__ R ld(const void* p, int o) { return ((const T*)p)[o]; }
     __device__ static __forceinline__ R cvt(T v) { return v; }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = v; }
+    __device__ static __forceinline__ T enc(R v) { return v; }
 };
 // FP16 holds h_i * 2^14: at low Mach numbers h_i is 1e-7..1e-4, below FP16's
 // smallest normal number (6.1e-5), where the subnormal spacing (6e-8) would cost
@@ -200,6 +206,12 @@ struct Store<ST_F16> {
     __device__ static __forceinline__ R ld(const void* p, int o) { return __half2float(((const T*)p)[o]); }
     __device__ static __forceinline__ R cvt(T v) { return __half2float(v); }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2half_rn(v); }
+    __device__ static __forceinline__ T enc(R v) { return __float2half_rn(v); }
+    // stochastic rounding: the 13 bits FP16 drops from a normal FP32 significand,
+    // plus the top 13 bits of the random word `r`, truncated
+    __device__ static __forceinline__ T enc_sr(R v, uint32_t r) {
+        return __float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19)));
+    }
 };
 template <>
 struct Store<ST_BF16> {
@@ -211,6 +223,10 @@ struct Store<ST_BF16> {
     __device__ static __forceinline__ R ld(const void* p, int o) { return __bfloat162float(((const T*)p)[o]); }
     __device__ static __forceinline__ R cvt(T v) { return __bfloat162float(v); }
     __device__ static __forceinline__ void st(void* p, int o, R v) { ((T*)p)[o] = __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ T enc(R v) { return __float2bfloat16_rn(v); }
+    __device__ static __forceinline__ T enc_sr(R v, uint32_t r) {
+        return __float2bfloat16_rz(__uint_as_float(__float_as_uint(v) + (r >> 16)));
+    }
 };
 
 // ---- node geometry -----------------------------------------------------------
@@ -219,7 +235,9 @@ struct Store<ST_BF16> {
 struct Geo {
     int x, y, z;
     int xm, xp, ym, yp, zm, zp;
-    int cell;
+    int cell;   // node index x + nx * (y + ny * z)
+    int slot;   // index of the node's populations in the planes: the node index (dense
+                // layouts) or the fluid-node index (sparse layout)
     int oxm, oxp, oym, oyp, ozm, ozp;
     __device__ __forceinline__ void offsets(const StepParams& P) {
         oxm = xm - x;
@@ -602,7 +620,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
             if constexpr (leaves<L>(i, F)) {
-                R v = S::unsc(S::ld(P.srcp[i], g.cell));
+                R v = S::unsc(S::ld(P.srcp[i], g.slot));
                 if (kind == BC_BOUNCE_BACK) {
                     R cu = R(0);
 #pragma unroll
@@ -631,7 +649,7 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
 #pragma unroll
                 for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
                 // with h = f - w: h[ibar] = -h*[i] + 2 w (rho_w (...) - 1)
-                f[L::qbar(i)] = -S::unsc(S::ld(P.srcp[i], g.cell)) +
+                f[L::qbar(i)] = -S::unsc(S::ld(P.srcp[i], g.slot)) +
                                 R(2) * R(L::w(i)) * (rw * (R(1) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3)) -
                                                      (S::DEV ? R(1) : R(0)));
             }
@@ -668,7 +686,7 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
     if (kind == SBC_BB_NO_FLUX) {
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (leaves<L>(i, F)) gg[L::qbar(i)] = ((const R*)P.gsrcp[i])[g.cell];
+            if constexpr (leaves<L>(i, F)) gg[L::qbar(i)] = ((const R*)P.gsrcp[i])[g.slot];
         });
         return;
     }
@@ -695,7 +713,7 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
 #pragma unroll
             for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
             const R ge = R(L::w(i)) * sval * (R(1) + cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
-            gg[L::qbar(i)] = -((const R*)P.gsrcp[i])[g.cell] + R(2) * ge;
+            gg[L::qbar(i)] = -((const R*)P.gsrcp[i])[g.slot] + R(2) * ge;
         }
     });
 }
@@ -769,16 +787,179 @@ __device__ __forceinline__ double fma_rn(double a, double b, double c) { return 
 // Equilibrium, collision and store of the post-collision populations.  BGK and
 // TRT are evaluated one direction (BGK) or one opposite pair (TRT) at a time
 // and stored at once, so only f[] stays live; MRT needs all moments together.
-template <int VS, int COLL, int ST>
+// ---- central-moment collision (D2Q9, D3Q27: tensor-product velocity sets) ----------
+// An engine extension: the reference has no D3Q27 collision at all
+// (src/velocity_set.rs:168).  The populations are transformed to central moments
+// about the node velocity u by three passes of 3-point transforms, one per axis
+// (the factorised "chimera" transform of Geier et al., Comput. Math. Appl. 70
+// (2015) 507-547): along an axis with velocities (-1, 0, +1), raw moments
+// M0 = f- + f0 + f+, M1 = f+ - f-, M2 = f+ + f-, then central ones k0 = M0,
+// k1 = M1 - u M0, k2 = M2 - 2 u M1 + u^2 M0.  The moments relax towards those of
+// the product-form equilibrium rho * c(a) c(b) c(c), c = (1, 0, 1/3):
+//   order 0 conserved; order 1 reflected (k1 -> -k1: no change without a force,
+//   adds F with the half-force velocity shift);
+//   order 2: the deviatoric normal parts and the off-diagonal ones at omega = 1/tau
+//   (shear viscosity (tau - 1/2) / 3), the trace at omega_bulk;
+//   orders 3, 4, 5, 6 at omega_3 .. omega_6 (default 1: full relaxation to the
+//   equilibrium, which is what keeps the scheme stable at tau close to 1/2).
+// The inverse transform runs the passes backwards: M1 = k1 + u k0,
+// M2 = k2 + 2 u k1 + u^2 k0, f+ = (M2 + M1) / 2, f- = (M2 - M1) / 2, f0 = M0 - M2.
+// With deviation storage the transform runs on h = f - w: the weights' central
+// moments about u are the products of (1, -u_a, 1/3 + u_a^2), subtracted from the
+// equilibrium targets, so every quantity stays small (no rounding against w).
+template <class L>
+__host__ __device__ constexpr int cm_pos(int i) {
+    return (L::c(i, 0) + 1) + 3 * (L::c(i, 1) + 1) + (L::D == 3 ? 9 * (L::c(i, 2) + 1) : 0);
+}
+
+template <int VS, int ST, class StoreFn>
+__device__ __forceinline__ void central_collide(const KParams<VS>& P, typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                                typename Store<ST>::R rho, const typename Store<ST>::R* u,
+                                                StoreFn&& store) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int D = L::D, Q = L::Q;
+    static_assert(Q == 9 || Q == 27, "central moments need a tensor-product velocity set");
+    constexpr bool DEV = S::DEV;
+    R v[Q];
+    sfor<Q>([&](auto I) { v[cm_pos<L>(I)] = S::unsc(f[I]); });
+    // forward passes: axis A (stride 1, 3, 9), velocities -1, 0, +1 at offsets 0, s, 2s
+    sfor<D>([&](auto A) {
+        constexpr int s = A == 0 ? 1 : (A == 1 ? 3 : 9);
+        const R ua = u[A];
+        sfor<Q / 3>([&](auto J) {
+            constexpr int j = J;
+            constexpr int base = (j % s) + (j / s) * 3 * s;   // line j of axis A
+            const R fm = v[base], f0 = v[base + s], fp = v[base + 2 * s];
+            const R M0 = fm + f0 + fp, M1 = fp - fm, M2 = fp + fm;
+            v[base] = M0;
+            v[base + s] = M1 - ua * M0;
+            v[base + 2 * s] = M2 - R(2) * ua * M1 + ua * ua * M0;
+        });
+    });
+    // relaxation; k(a, b, c) sits at a + 3 b + 9 c (a, b, c = moment order per axis)
+    const R om = R(P.omega), ob = R(P.rates[0]);
+    const R w3 = R(P.rates[1]), w4 = R(P.rates[2]), w5 = R(P.rates[3]), w6 = R(P.rates[4]);
+    auto mfac = [&](int a, int ax) -> R {   // weights' central moment factor along axis ax
+        return a == 0 ? R(1) : (a == 1 ? -u[ax] : R(1.0 / 3.0) + u[ax] * u[ax]);
+    };
+    auto eq = [&](int a, int b, int c) -> R {   // equilibrium target (minus the weights' part)
+        auto cf = [](int o) { return o == 0 ? 1.0 : (o == 1 ? 0.0 : 1.0 / 3.0); };
+        R e = rho * R(cf(a) * cf(b) * cf(c));
+        if constexpr (DEV) e -= mfac(a, 0) * mfac(b, 1) * (D == 3 ? mfac(c, 2) : R(1));
+        return e;
+    };
+    // first order: reflection about the equilibrium value (-u with deviations, 0 otherwise)
+    sfor<D>([&](auto A) {
+        constexpr int pos = A == 0 ? 1 : (A == 1 ? 3 : 9);
+        v[pos] = (DEV ? R(2) * u[A] : R(0)) - v[pos];
+    });
+    // second order
+    {
+        constexpr int pxx = 2, pyy = 6, pzz = 18;
+        const R dxx = v[pxx] - eq(2, 0, 0), dyy = v[pyy] - eq(0, 2, 0);
+        if constexpr (D == 3) {
+            const R dzz = v[pzz] - eq(0, 0, 2);
+            const R tr = (R(1) - ob) * (dxx + dyy + dzz);
+            const R dxy = (R(1) - om) * (dxx - dyy), dxz = (R(1) - om) * (dxx - dzz);
+            const R nxx = (tr + dxy + dxz) * R(1.0 / 3.0);
+            v[pxx] = eq(2, 0, 0) + nxx;
+            v[pyy] = eq(0, 2, 0) + (nxx - dxy);
+            v[pzz] = eq(0, 0, 2) + (nxx - dxz);
+            v[4] = eq(1, 1, 0) + (R(1) - om) * (v[4] - eq(1, 1, 0));      // (1,1,0)
+            v[10] = eq(1, 0, 1) + (R(1) - om) * (v[10] - eq(1, 0, 1));    // (1,0,1)
+            v[12] = eq(0, 1, 1) + (R(1) - om) * (v[12] - eq(0, 1, 1));    // (0,1,1)
+        } else {
+            const R tr = (R(1) - ob) * (dxx + dyy), dxy = (R(1) - om) * (dxx - dyy);
+            v[pxx] = eq(2, 0, 0) + R(0.5) * (tr + dxy);
+            v[pyy] = eq(0, 2, 0) + R(0.5) * (tr - dxy);
+            v[4] = eq(1, 1, 0) + (R(1) - om) * (v[4] - eq(1, 1, 0));
+        }
+    }
+    // orders 3..6
+    sfor<Q>([&](auto Pp) {
+        constexpr int p = Pp;
+        constexpr int a = p % 3, b = (p / 3) % 3, c = p / 9;
+        constexpr int ord = a + b + c;
+        if constexpr (ord >= 3) {
+            const R w = ord == 3 ? w3 : (ord == 4 ? w4 : (ord == 5 ? w5 : w6));
+            const R e = eq(a, b, c);
+            v[p] = e + (R(1) - w) * (v[p] - e);
+        }
+    });
+    // backward passes, last axis first
+    sfor<D>([&](auto AA) {
+        constexpr int A = D - 1 - AA;
+        constexpr int s = A == 0 ? 1 : (A == 1 ? 3 : 9);
+        const R ua = u[A];
+        sfor<Q / 3>([&](auto J) {
+            constexpr int j = J;
+            constexpr int base = (j % s) + (j / s) * 3 * s;
+            const R k0 = v[base], k1 = v[base + s], k2 = v[base + 2 * s];
+            const R M1 = k1 + ua * k0, M2 = k2 + R(2) * ua * k1 + ua * ua * k0;
+            v[base] = (M2 - M1) * R(0.5);
+            v[base + s] = k0 - M2;
+            v[base + 2 * s] = (M2 + M1) * R(0.5);
+        });
+    });
+    sfor<Q>([&](auto I) { store(I, S::sc(v[cm_pos<L>(I)])); });
+}
+
+// 32-bit integer hash (two multiply / xor-shift rounds): the seed of a node's
+// stochastic rounding in one time step.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+// Odd multipliers that spread a node's seed over its directions.
+__host__ __device__ constexpr uint32_t sr_mult(int i) { return 0x9e3779b1u + 0x632be5abu * (uint32_t)(2 * i); }
+
+// `put(IC<i>, t)` stores the post-collision value of direction i, already in the
+// storage type.  `nseed` seeds the stochastic rounding of 16-bit storage.
+template <int VS, int COLL, int ST, class Put>
 __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Store<ST>::R (&f)[Lat<VS>::Q],
                                               typename Store<ST>::R rho, typename Store<ST>::R dr,
                                               const typename Store<ST>::R* u, typename Store<ST>::R uu,
-                                              const typename Store<ST>::R* F, bool force, long long cell) {
+                                              const typename Store<ST>::R* F, bool force, uint32_t nseed,
+                                              Put&& put) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
     constexpr int Q = L::Q;
     constexpr bool DEV = S::DEV;
+    // 16-bit storage rounds every stored value to 11 (FP16) or 8 (BF16) significant
+    // bits.  Two measures keep those roundings from adding up over the steps:
+    // - the mass they add or remove is put back into the rest population, stored
+    //   last, so the node's outgoing mass carries only the rest population's own
+    //   rounding (its value is small, so is its ulp); mass is conserved, nothing
+    //   damps a mass error, and density errors drive spurious pressure-gradient flow;
+    // - stochastic rounding (P.sround): near a steady state the populations repeat
+    //   from step to step, and round-to-nearest then repeats the same error at every
+    //   step, a persistent spurious momentum source; rounding up or down with
+    //   probability given by the distance makes the error zero-mean, so it averages
+    //   out instead of accumulating.
+    constexpr bool SIXTEEN = ST == ST_F16 || ST == ST_BF16;
+    R merr = R(0), v0 = R(0);
+    auto store = [&](auto I, R v) {
+        using T = typename S::T;
+        if constexpr (SIXTEEN) {
+            if constexpr (int(I) == 0) {
+                v0 = v;   // stored after the others
+                return;
+            } else {
+                const T t = P.sround ? S::enc_sr(v, nseed * sr_mult(int(I))) : S::enc(v);
+                merr += v - S::cvt(t);
+                put(I, t);
+            }
+        } else {
+            put(I, S::enc(v));
+        }
+    };
     if constexpr (COLL == COLL_BGK) {
         // f[] and the result are scaled by the storage scale: so are w1 and cb
         const R w1 = S::sc(R(P.omega)), w0 = R(1) - R(P.omega);
@@ -787,7 +968,7 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
             constexpr int i = I;
             R v = w0 * f[i] + w1 * eq_i<L, DEV, R>(i, rho, dr, u, uu);
             if (force) v += cb * guo_i<L, R>(i, u, F);
-            S::st(P.dstp[i], cell, v);
+            store(IC<i>{}, v);
         });
     } else if constexpr (COLL == COLL_TRT) {
         const R wp = R(P.op), wm = R(P.om);
@@ -824,10 +1005,12 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
                     vi += cp * R(0.5) * (si + sb) + cm * R(0.5) * (si - sb);
                     vb += cp * R(0.5) * (sb + si) + cm * R(0.5) * (sb - si);
                 }
-                S::st(P.dstp[i], cell, vi);
-                if constexpr (i != ib) S::st(P.dstp[ib], cell, vb);
+                store(IC<i>{}, vi);
+                if constexpr (i != ib) store(IC<ib>{}, vb);
             }
         });
+    } else if constexpr (COLL == COLL_CENTRAL) {
+        if constexpr (L::Q == 9 || L::Q == 27) central_collide<VS, ST>(P, f, rho, u, store);
     } else if constexpr (VS == VS_D3Q27) {
         // population-space MRT, f* = f - Lambda (f - f_eq) (+ the Guo source in physics
         // mode): only the Q deviations e = f - f_eq (+ s/2) stay live through the
@@ -848,14 +1031,18 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
             sfor<Q>([&](auto J) { acc += lam_at<VS, R>(P, i * Q + J) * e[J]; });
             R v = eq_i<L, DEV, R>(i, rho, dr, u, uu) + e[i] - acc;
             if (src) v += R(0.5) * guo_i<L, R>(i, u, F);
-            S::st(P.dstp[i], cell, S::sc(v));
+            store(IC<i>{}, S::sc(v));
         });
     } else {
         R fe[Q];
         sfor<Q>([&](auto I) { fe[I] = eq_i<L, DEV, R>(I, rho, dr, u, uu); });
         sfor<Q>([&](auto I) { f[I] = S::unsc(f[I]); });
         collide<VS, COLL, DEV, R>(P, f, fe, rho, dr, u, F, force, P.tau, P.omega, P.op, P.om, P.rates, P.compat);
-        sfor<Q>([&](auto I) { S::st(P.dstp[I], cell, S::sc(f[I])); });
+        sfor<Q>([&](auto I) { store(I, S::sc(f[I])); });
+    }
+    if constexpr (SIXTEEN) {
+        const R v = v0 + merr;
+        put(IC<0>{}, P.sround ? S::enc_sr(v, nseed * sr_mult(0)) : S::enc(v));
     }
 }
 
@@ -910,13 +1097,12 @@ __device__ __forceinline__ bool gated_off(const StepParams& P) {
 
 // Everything a fluid node does after its populations were pulled: face BCs,
 // moments, residual/observe/face-layer outputs, collision + store, and the
-// scalar step.  Shared by the single-pass sweep and the pipelined sweep.
-// `pidx` is the index of the node's populations in the planes: the node index
-// for the dense layouts, the fluid-node index for the sparse layout.
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
-__device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo& g, uint32_t mk,
-                                                typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                                typename Store<ST>::R* gg, double (&racc)[5], long long pidx) {
+// scalar step.  Shared by every sweep.
+// `put` stores the post-collision populations (see collide_store).
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class Put>
+__device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                                 typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                                 typename Store<ST>::R* gg, double (&racc)[5], Put&& put) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
@@ -1014,7 +1200,8 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
         // ---- equilibrium + collision --------------------------------------------
         R uu = R(0);
         sfor<D>([&](auto A) { uu += u[A] * u[A]; });
-        collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, pidx);
+        const uint32_t nseed = (ST == ST_F16 || ST == ST_BF16) ? mix32((uint32_t)g.slot ^ (P.tstep * 0x9e3779b9u)) : 0u;
+        collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, nseed, put);
 
         if constexpr (SCALAR) {
             // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
@@ -1040,13 +1227,26 @@ __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo&
                 });
                 sfor<Q>([&](auto I) { gg[I] = out[I]; });
             }
-            sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = gg[I]; });
+            sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.slot] = gg[I]; });
             if (P.s_ads && bb) {
                 ((R*)P.qads)[g.cell] = q;
                 ((R*)P.cprev)[g.cell] = cval;
             }
         }
     }
+}
+
+// The A/B layouts: the post-collision populations go to slot `pidx` of the
+// destination planes (the node index for the dense layouts, the fluid-node index
+// for the sparse layout).
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                                typename Store<ST>::R (&f)[Lat<VS>::Q],
+                                                typename Store<ST>::R* gg, double (&racc)[5], long long pidx) {
+    using S = Store<ST>;
+    process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc, [&](auto I, typename S::T v) {
+        ((typename S::T*)P.dstp[I])[pidx] = v;
+    });
 }
 
 template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
@@ -1065,7 +1265,9 @@ __device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g,
 // Light kernels (BGK/TRT on D2Q9/D3Q19, FP32 compute, no scalar) are held to 64 registers
 // so that at least 1024 threads fit on an SM; the others may use 128.
 template <int VS, int COLL, int ST, bool SCALAR>
-constexpr int light_kernel() { return COLL != COLL_MRT && VS != VS_D3Q27 && !SCALAR && ST != ST_F64 ? 2 : 1; }
+constexpr int light_kernel() {
+    return COLL != COLL_MRT && COLL != COLL_CENTRAL && VS != VS_D3Q27 && !SCALAR && ST != ST_F64 ? 2 : 1;
+}
 
 template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, bool STAGE>
 __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_kernel<VS, COLL, ST, SCALAR>())
@@ -1097,6 +1299,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         if (!inside) g.x = 0;
     }
     g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+    g.slot = g.cell;
     g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
     g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
     g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
@@ -1241,6 +1444,7 @@ __global__ void __launch_bounds__(256, ST == ST_F64 ? 2 : 4) k_step_list(const K
     const uint32_t e = valid ? P.list[t] : 0u;
     Geo g;
     g.cell = (int)(e & 0x3fffffffu);
+    g.slot = g.cell;
     if (e >> 31) {
         // coordinates by a double-precision reciprocal plus a +-1 correction
         // (exact for indices < 2^31), much cheaper than integer division
@@ -1399,6 +1603,7 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
                 const bool inside = g.x < P.nx;
                 if (!inside) g.x = 0;
                 g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+                g.slot = g.cell;
                 g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
                 g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
                 g.offsets(P);
@@ -1451,92 +1656,192 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
 // the row.  A sentinel row after the last holds .y = number of fluid nodes.
 // Linked directions (solid source, or a folded no-slip wall) read the node's own
 // f*[ibar], as the dense sweeps do.
+// The sparse layout's pull source of direction i for fluid node k at g: the
+// fluid slot of x - c_i (meaningful unless the link bit of ibar is set).  Word w
+// of row (y', z') holds the fluid bits of x in [32w, 32w + 32) (.x) and the fluid
+// index of the first fluid node at or after x = 32w (.y); with p = .y + popc(.x &
+// bits below x), the three directions sharing the row read idx(x - 1) = p - 1,
+// idx(x) = p and idx(x + 1) = p + (bit x of the row); the periodic wrap in x
+// (WRAP: some lane of the warp is at a row end) reads the first index of the next
+// row, or of the row.
+template <class L, int i, bool WRAP>
+__device__ __forceinline__ int sparse_source(const StepParams& P, const Geo& g, int k) {
+    constexpr int D = L::D;
+    constexpr int cx = L::c(i, 0), cy = L::c(i, 1), cz = D == 3 ? L::c(i, 2) : 0;
+    const int W = P.rw_w;
+    const int w = g.x >> 5, b = g.x & 31;
+    const unsigned below = (1u << b) - 1u;
+    const int row = g.y + P.ny * g.z;
+    int idx;
+    if constexpr (cy == 0 && cz == 0) {
+        if constexpr (cx == 0) idx = k;
+        else if constexpr (cx == 1)
+            idx = (WRAP && g.x == 0) ? (int)P.rw[((unsigned)row + 1u) * (unsigned)W].y - 1 : k - 1;
+        else idx = (WRAP && g.x == P.nx - 1) ? (int)P.rw[(unsigned)row * (unsigned)W].y : k + 1;
+    } else {
+        const int ys = cy > 0 ? g.ym : (cy < 0 ? g.yp : g.y);
+        const int zs = cz > 0 ? g.zm : (cz < 0 ? g.zp : g.z);
+        // row-word indices stay below (rows + 1) * W <= N / 32 + 2 rows + 1 < 2^32
+        const unsigned r2 = (unsigned)ys + (unsigned)P.ny * (unsigned)zs;
+        const uint2 v = P.rw[r2 * (unsigned)W + (unsigned)w];
+        const int p = (int)v.y + __popc(v.x & below);
+        if constexpr (cx == 0) idx = p;
+        else if constexpr (cx == 1) idx = (WRAP && g.x == 0) ? (int)P.rw[(r2 + 1u) * (unsigned)W].y - 1 : p - 1;
+        else idx = (WRAP && g.x == P.nx - 1) ? (int)P.rw[r2 * (unsigned)W].y : p + (int)((v.x >> b) & 1u);
+    }
+    return idx;
+}
+
+// In-place streaming (AA pattern) in the sparse layout: one population buffer A,
+// plane i holding direction i per fluid slot.  The state between launches
+// alternates between two placements of the post-collision populations f*:
+//  - an even step (t even) reads f_i(x) = A[i][x] and stores f*_i(x) into the
+//    node's own slot of the opposite plane, A[ibar][x];
+//  - an odd step reads f_i(x) = A[ibar][x - c_i] (the value the neighbour x - c_i
+//    stored there one step before) and stores f*_i(x) into A[i][x + c_i], where
+//    the next even step of node x + c_i reads it.
+// A neighbour that is solid (a link) turns both into the node's own slots:
+// f_i(x) = A[i][x] (its own f*_ibar of the previous even step) and f*_i(x) goes
+// to A[ibar][x] (read as f_ibar(x) by the next even step): half-way bounce-back,
+// src/lib.rs:154-165.  In an odd step, the slot that direction i is read from is
+// the slot that f*_ibar is stored to, and no other node touches it, so each slot
+// is read once and written once per step and no step needs a second buffer.  The
+// values pulled and the arithmetic are those of the A/B pull sweep, so both give
+// the same bits; an even step needs no neighbour index, mask word or list entry.
+//
+// Push (SWEEP_PUSH, two buffers): the state between launches is the post-stream
+// field f_t itself.  A step reads f_t(x) from the node's own slots (contiguous,
+// no neighbour index on the load path), collides, and stores f*_i(x) into slot
+// x + c_i of plane i of the other buffer (plane ibar of its own slot when x + c_i
+// is solid), which is f_{t+1}.  The values and the arithmetic are again those of
+// the pull sweep.
+constexpr int SWEEP_PULL = 0, SWEEP_AA_EVEN = 1, SWEEP_AA_ODD = 2, SWEEP_PUSH = 3;
+
 // One fluid node of the sparse sweep (k64 = its fluid index; lanes past the
-// last fluid node only take part in the block reduction).
-template <int VS, int COLL, int ST>
-__device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k64, uint32_t e, uint32_t mk,
-                                               double (&racc)[5]) {
+// last fluid node only take part in the block reduction).  `e` and `mk` (its
+// list entry and mask word) are read lazily: an in-place even step that writes
+// no moments needs neither.
+template <int VS, int COLL, int ST, int MODE>
+__device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k64, const uint32_t* ep,
+                                               const uint32_t* mp, double (&racc)[5]) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
+    using T = typename S::T;
     constexpr int Q = L::Q, D = L::D;
     const bool valid = k64 < P.nlist;
     const int k = valid ? (int)k64 : (int)(P.nlist - 1);
+    // an in-place even step reads the node's own slots: coordinates only for outputs
+    const bool need_geo = MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom;
     Geo g;
-    if (P.packed) {   // coordinates packed at set-up: no division
-        g.x = (int)(e & 2047u);
-        g.y = (int)((e >> 11) & 2047u);
-        g.z = (int)(e >> 22);
-        g.cell = g.x + P.nx * (g.y + P.ny * g.z);
-    } else {
-        auto divq = [](int n, int d, double inv) {
-            int q = (int)((double)n * inv);
-            q -= ((long long)q * d > n);
-            q += ((long long)(q + 1) * d <= n);
-            return q;
-        };
-        g.cell = (int)e;
-        const int row = divq(g.cell, P.nx, P.inv_nx);
-        g.x = g.cell - row * P.nx;
-        g.z = divq(row, P.ny, P.inv_ny);
-        g.y = row - g.z * P.ny;
+    g.x = g.y = g.z = g.cell = 0;
+    g.slot = k;
+    uint32_t mk = 0;
+    if (need_geo) {
+        const uint32_t e = *ep;
+        if (MODE != SWEEP_AA_EVEN) mk = *mp;
+        if (P.packed) {   // coordinates packed at set-up: no division
+            g.x = (int)(e & 2047u);
+            g.y = (int)((e >> 11) & 2047u);
+            g.z = (int)(e >> 22);
+            g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+        } else {
+            auto divq = [](int n, int d, double inv) {
+                int q = (int)((double)n * inv);
+                q -= ((long long)q * d > n);
+                q += ((long long)(q + 1) * d <= n);
+                return q;
+            };
+            g.cell = (int)e;
+            const int row = divq(g.cell, P.nx, P.inv_nx);
+            g.x = g.cell - row * P.nx;
+            g.z = divq(row, P.ny, P.inv_ny);
+            g.y = row - g.z * P.ny;
+        }
+        g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+        g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+        g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+        g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+        g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+        g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
     }
-    g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
-    g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
-    g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
-    g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
-    g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
-    g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
     if (!valid) return;
     R f[Q];
-    if (P.first) {
+    auto pull_index = [&](auto I, auto WRAP) -> int {
+        return sparse_source<L, int(I), decltype(WRAP)::value != 0>(P, g, k);
+    };
+    if constexpr (MODE == SWEEP_AA_EVEN) {
         sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
-    } else {
-        const int W = P.rw_w;
-        const int w = g.x >> 5, b = g.x & 31;
-        const unsigned below = (1u << b) - 1u;
-        const int row = g.y + P.ny * g.z;
-        // WRAP: the periodic wrap in x (x = 0 pulls from x = nx - 1 and x = nx - 1
-        // from x = 0) needs the first index of a row; a warp with no lane at a row
-        // end pulls without that code
-        auto pull = [&](auto WRAP) {
-            sfor<Q>([&](auto I) {
+        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
+            ((T*)P.dstp[L::qbar(I)])[k] = v;
+        });
+    } else if constexpr (MODE == SWEEP_PUSH) {
+        sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
+        auto body = [&](auto WRAP) {
+            process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
                 constexpr int i = I, ib = L::qbar(i);
-                constexpr int cx = L::c(i, 0), cy = L::c(i, 1), cz = D == 3 ? L::c(i, 2) : 0;
-                constexpr bool wrap = decltype(WRAP)::value != 0;
-                int idx;
-                if constexpr (cy == 0 && cz == 0) {
-                    if constexpr (cx == 0) idx = k;
-                    else if constexpr (cx == 1)
-                        idx = (wrap && g.x == 0) ? (int)P.rw[((unsigned)row + 1u) * (unsigned)W].y - 1 : k - 1;
-                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[(unsigned)row * (unsigned)W].y : k + 1;
+                if constexpr (i == 0) {
+                    ((T*)P.dstp[0])[k] = v;
                 } else {
-                    const int ys = cy > 0 ? g.ym : (cy < 0 ? g.yp : g.y);
-                    const int zs = cz > 0 ? g.zm : (cz < 0 ? g.zp : g.z);
-                    // row-word indices stay below (rows + 1) * W <= N / 32 + 2 rows + 1 < 2^32
-                    const unsigned r2 = (unsigned)ys + (unsigned)P.ny * (unsigned)zs;
-                    const uint2 v = P.rw[r2 * (unsigned)W + (unsigned)w];
-                    const int p = (int)v.y + __popc(v.x & below);
-                    if constexpr (cx == 0) idx = p;
-                    else if constexpr (cx == 1) idx = (wrap && g.x == 0) ? (int)P.rw[(r2 + 1u) * (unsigned)W].y - 1 : p - 1;
-                    else idx = (wrap && g.x == P.nx - 1) ? (int)P.rw[r2 * (unsigned)W].y : p + (int)((v.x >> b) & 1u);
+                    // x + c_i is the pull source of direction ibar
+                    const bool lk = (mk >> i) & 1u;
+                    const int idx = sparse_source<L, ib, decltype(WRAP)::value != 0>(P, g, k);
+                    ((T*)(lk ? P.dstp[ib] : P.dstp[i]))[lk ? k : idx] = v;
                 }
-                const bool lk = (mk >> ib) & 1u;
-                f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
             });
         };
-        // (a warp-uniform split on the link bits as well measured 3-5 % slower: the
-        // branch-free bounce-back select costs less than the extra code)
-        if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
-        else pull(IC<0>{});
+        if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) body(IC<1>{});
+        else body(IC<0>{});
+    } else if constexpr (MODE == SWEEP_AA_ODD) {
+        // element offsets from plane 0: read f_i there, store f*_ibar there (q * np < 2^32)
+        unsigned off[Q];
+        const unsigned np = (unsigned)P.np;
+        auto load = [&](auto WRAP) {
+            sfor<Q>([&](auto I) {
+                constexpr int i = I, ib = L::qbar(i);
+                if constexpr (i == 0) {
+                    off[0] = (unsigned)k;
+                } else {
+                    const bool lk = (mk >> ib) & 1u;
+                    const unsigned own = (unsigned)i * np + (unsigned)k;
+                    off[i] = lk ? own : (unsigned)ib * np + (unsigned)pull_index(I, WRAP);
+                }
+                f[i] = S::cvt(((const T*)P.srcp[0])[off[i]]);
+            });
+        };
+        if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) load(IC<1>{});
+        else load(IC<0>{});
+        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
+            ((T*)P.dstp[0])[off[L::qbar(I)]] = v;
+        });
+    } else {
+        if (P.first) {
+            sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
+        } else {
+            // WRAP: the periodic wrap in x (x = 0 pulls from x = nx - 1 and x = nx - 1
+            // from x = 0) needs the first index of a row; a warp with no lane at a row
+            // end pulls without that code
+            auto pull = [&](auto WRAP) {
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    const int idx = pull_index(I, WRAP);
+                    const bool lk = (mk >> ib) & 1u;
+                    f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
+                });
+            };
+            // (a warp-uniform split on the link bits as well measured 3-5 % slower: the
+            // branch-free bounce-back select costs less than the extra code)
+            if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
+            else pull(IC<0>{});
+        }
+        process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, k);
     }
-    process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, k);
 }
 
-template <int VS, int COLL, int ST>
+template <int VS, int COLL, int ST, int MODE = SWEEP_PULL>
 __device__ __forceinline__ void sparse_node(const KParams<VS>& P, long long k64, double (&racc)[5]) {
     const int k = k64 < P.nlist ? (int)k64 : (int)(P.nlist - 1);
-    sparse_node_at<VS, COLL, ST>(P, k64, P.list[k], P.fmask[k], racc);
+    sparse_node_at<VS, COLL, ST, MODE>(P, k64, P.list + k, P.fmask + k, racc);
 }
 
 // One bulk prefetch of a global range into L2 (16-byte aligned, size a multiple of 16).
@@ -1576,13 +1881,137 @@ __device__ __forceinline__ void sparse_prefetch(const KParams<VS>& P) {
     }
 }
 
-template <int VS, int COLL, int ST>
-__global__ void __launch_bounds__(256, 2 * light_kernel<VS, COLL, ST, false>()) k_step_sparse(const KParams<VS> P) {
+// An in-place odd step keeps the Q slot offsets of its loads for its stores: 80
+// registers (three blocks per SM) instead of the 64 of the other light sweeps.
+template <int VS, int COLL, int ST, int MODE>
+constexpr int sparse_blocks() {
+    return light_kernel<VS, COLL, ST, false>() == 2 ? (MODE == SWEEP_AA_ODD ? 3 : 4) : 2;
+}
+
+template <int VS, int COLL, int ST, int MODE>
+__global__ void __launch_bounds__(256, (sparse_blocks<VS, COLL, ST, MODE>())) k_step_sparse(const KParams<VS> P) {
     if (gated_off(P)) return;
-    sparse_prefetch<VS, ST>(P);
+    // an in-place even step reads only its own contiguous slots: nothing to prefetch
+    if (MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom) sparse_prefetch<VS, ST>(P);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const long long k = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    sparse_node<VS, COLL, ST>(P, k < P.kend ? k : P.nlist, racc);   // nlist: no update
+    sparse_node<VS, COLL, ST, MODE>(P, k < P.kend ? k : P.nlist, racc);   // nlist: no update
+    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+}
+
+// =================================================================== sparse sweep, faces and scalar
+// The sparse layout for lattices with explicit face BCs and/or a passive scalar
+// (a packed bed: Zou-He or moving-wall inlet, anti-bounce-back outlet, scalar
+// with Langmuir adsorption).  Thread k updates fluid node k as k_step_sparse
+// does, with two population buffers; the scalar populations live in the same
+// fluid slots and are pulled through the same source indices.  Face nodes run
+// apply_faces on their own slots; the nodes of a scalar outflow face are left to
+// the face pass (P.face_pass: one thread per position of face fp_face), which
+// finds a node's fluid slot through the row words.  Per-node side arrays
+// (adsorbed amount, previous scalar value, residual moments, face layers) stay
+// indexed by node, as in the dense layout.
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__global__ void __launch_bounds__(256, 2) k_step_sparse_fs(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    if (gated_off(P)) return;
+    Geo g;
+    uint32_t mk = M_SOLID;
+    bool valid;
+    int k = 0;
+    if (FACEBC && P.face_pass) {
+        const int F = P.fp_face;
+        const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        valid = pos < P.pb_plane[F];
+        const long long pp = valid ? pos : 0;
+        if (F < 2) { g.x = F == 0 ? 0 : P.nx - 1; g.y = (int)(pp % P.ny); g.z = (int)(pp / P.ny); }
+        else if (F < 4) { g.y = F == 2 ? 0 : P.ny - 1; g.x = (int)(pp % P.nx); g.z = (int)(pp / P.nx); }
+        else { g.z = F == 4 ? 0 : P.nz - 1; g.x = (int)(pp % P.nx); g.y = (int)(pp / P.nx); }
+        g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+        mk = valid ? P.mask[g.cell] : M_SOLID;
+        valid = valid && !(mk & M_SOLID) && (mk & M_SKIP);
+        if (valid) {
+            const uint2 v = P.rw[(unsigned)(g.y + P.ny * g.z) * (unsigned)P.rw_w + (unsigned)(g.x >> 5)];
+            k = (int)v.y + __popc(v.x & ((1u << (g.x & 31)) - 1u));
+        }
+    } else {
+        const long long k64 = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        valid = k64 < P.kend;
+        k = valid ? (int)k64 : (int)(P.kend - 1);
+        const uint32_t e = P.list[k];
+        mk = P.fmask[k];
+        if (P.packed) {
+            g.x = (int)(e & 2047u);
+            g.y = (int)((e >> 11) & 2047u);
+            g.z = (int)(e >> 22);
+            g.cell = g.x + P.nx * (g.y + P.ny * g.z);
+        } else {
+            auto divq = [](int n, int d, double inv) {
+                int q = (int)((double)n * inv);
+                q -= ((long long)q * d > n);
+                q += ((long long)(q + 1) * d <= n);
+                return q;
+            };
+            g.cell = (int)e;
+            const int row = divq(g.cell, P.nx, P.inv_nx);
+            g.x = g.cell - row * P.nx;
+            g.z = divq(row, P.ny, P.inv_ny);
+            g.y = row - g.z * P.ny;
+        }
+        if (FACEBC) valid = valid && !(mk & M_SKIP);
+    }
+    g.slot = k;
+    g.xm = g.x == 0 ? P.nx - 1 : g.x - 1;
+    g.xp = g.x == P.nx - 1 ? 0 : g.x + 1;
+    g.ym = g.y == 0 ? P.ny - 1 : g.y - 1;
+    g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
+    g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
+    g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
+    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+        R f[Q];
+        R gg[SCALAR ? Q : 1];
+        if (P.first) {
+            sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
+            if constexpr (SCALAR) sfor<Q>([&](auto I) { gg[I] = ((const R*)P.gsrcp[I])[k]; });
+        } else {
+            // pull + inner bounce-back (src/lib.rs:141-165); the scalar's inner BC
+            // (src/passive_scalar/lattice.rs:274-297) on the same source index
+            auto pull = [&](auto WRAP) {
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    const int idx = sparse_source<L, i, decltype(WRAP)::value != 0>(P, g, k);
+                    const bool lk = (mk >> ib) & 1u;
+                    f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
+                    if constexpr (SCALAR) {
+                        if (lk) {
+                            const R own = ((const R*)P.gsrcp[ib])[k];
+                            if (P.s_inner == 1) {
+                                gg[i] = own;   // InnerBounceBack
+                            } else {           // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
+                                R cs = R(P.c_solid);
+                                if (P.c_init) {   // the solid neighbour's initial value (periodic)
+                                    const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
+                                    const int ys = L::c(i, 1) > 0 ? g.ym : (L::c(i, 1) < 0 ? g.yp : g.y);
+                                    const int zs = D == 3 ? (L::c(i, 2) > 0 ? g.zm : (L::c(i, 2) < 0 ? g.zp : g.z)) : 0;
+                                    cs = R(P.c_init[xs + (long long)P.nx * (ys + (long long)P.ny * zs)]);
+                                }
+                                gg[i] = -own + R(2) * R(L::w(ib)) * cs;
+                            }
+                        } else {
+                            gg[i] = ((const R*)P.gsrcp[i])[idx];
+                        }
+                    }
+                });
+            };
+            if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
+            else pull(IC<0>{});
+        }
+        process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc,
+                                                        [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[k] = v; });
+    }
     if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
 }
 

@@ -1,13 +1,13 @@
 // noalloc.cu -- lbf_inventory_noalloc: FP64 fluid-node sums with no device allocation.
 //
 // Some callers cannot allocate device memory at the moment they need a
-// reduction: a host application that records its solver loop into a CUDA graph
-// (allocation calls are not allowed while a stream is being captured), a
-// service that reserved all of HBM for lattices up front and runs with a fixed
-// memory budget, or an embedding framework whose own caching allocator owns the
-// device memory.  For them this entry point sums caller-owned device arrays
-// using a scratch array that lives in the library's static device memory, so a
-// call performs no cudaMalloc, cudaFree or other allocating call.
+// reduction: a service that reserved all of HBM for lattices up front and runs
+// with a fixed memory budget (an allocation would fail, or evict a lattice), or
+// an embedding framework whose own caching allocator owns the device memory (an
+// allocation behind its back breaks its accounting).  For them this entry point
+// sums caller-owned device arrays using a scratch array that lives in the
+// library's static device memory, so a call performs no cudaMalloc, cudaFree or
+// other allocating call.
 //
 // The scratch array is a file-scope __device__ array of NSLOT x NACC doubles
 // (16 KiB).  Each GPU that loads the library holds one copy until the process
@@ -16,8 +16,11 @@
 // GPU (different streams without ordering) race on it and give wrong sums.
 //
 // Its device address is looked up once per device with cudaGetSymbolAddress,
-// with that device current, on the first call made on that device; make that
-// first call before any stream capture starts.
+// with that device current, on the first call made on that device; that first
+// call also loads the four kernels below, so that no later call loads code.
+// Make that first call before any stream capture starts.  The cached address
+// belongs to the device's primary context: after cudaDeviceReset the next call
+// must not be made (the address would be stale).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -79,6 +82,14 @@ lbf_status scratch_for_current_device(double** out) {
         e = cudaGetSymbolAddress((void**)&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p)
             return na_fail(LBF_EDEVICE, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        // load every kernel of this entry point now (module loading is lazy by default)
+        cudaFuncAttributes fa;
+        const void* fns[4] = {(const void*)k_clear_scratch, (const void*)k_inventory_class<2>,
+                              (const void*)k_inventory_class<3>, (const void*)k_sum_slots};
+        for (const void* fn : fns) {
+            e = cudaFuncGetAttributes(&fa, fn);
+            if (e != cudaSuccess) return na_fail(LBF_EDEVICE, std::string("kernel load: ") + cudaGetErrorString(e));
+        }
         g_scratch_ptr[dev] = p;
     }
     *out = g_scratch_ptr[dev];

@@ -1,0 +1,6 @@
+// Sparse-layout step kernels with explicit faces and the scalar: D2Q9, BGK.
+#include "dispatch.cuh"
+
+namespace lbf {
+LBF_INSTANTIATE_SPARSE_FS(VS_D2Q9, COLL_BGK)
+}  // namespace lbf

@@ -1,0 +1,6 @@
+// Sparse-layout step kernels with explicit faces and the scalar: D3Q19, MRT.
+#include "dispatch.cuh"
+
+namespace lbf {
+LBF_INSTANTIATE_SPARSE_FS(VS_D3Q19, COLL_MRT)
+}  // namespace lbf

@@ -2,5 +2,5 @@
 #include "dispatch.cuh"
 
 namespace lbf {
-LBF_INSTANTIATE(VS_D2Q9)
+LBF_INSTANTIATE(VS_D2Q9, 1)
 }  // namespace lbf

@@ -2,5 +2,5 @@
 #include "dispatch.cuh"
 
 namespace lbf {
-LBF_INSTANTIATE(VS_D3Q19)
+LBF_INSTANTIATE(VS_D3Q19, 0)
 }  // namespace lbf

@@ -2,5 +2,5 @@
 #include "dispatch.cuh"
 
 namespace lbf {
-LBF_INSTANTIATE(VS_D3Q27)
+LBF_INSTANTIATE(VS_D3Q27, 1)
 }  // namespace lbf

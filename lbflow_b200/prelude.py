@@ -4,7 +4,7 @@ from . import momentum, passive_scalar  # noqa: F401
 from . import momentum as m  # noqa: F401
 from . import passive_scalar as ps  # noqa: F401
 from .core import BGK, MRT, TRT, BoundaryFace, CollisionOperator, NodeType, VelocitySet  # noqa: F401
-from .core import Compat, Storage  # noqa: F401
+from .core import CentralMoment, Compat, Storage  # noqa: F401
 from .momentum import InitialDensity, InitialVelocity, NodeTypes  # noqa: F401
 from .momentum import FromBounceBackMapFile, OnlyFluidNodes  # noqa: F401
 from .passive_scalar import AdsorptionParameters, InitialScalarValue, Langmuir  # noqa: F401

@@ -545,6 +545,80 @@ void m_equilibrium(Domain& D) {
         equilibrium(D.vs, D.rho[idx], &D.u[idx * D.d], &D.feq[idx * D.q]);
     }
 }
+// Central-moment collision of the tensor-product sets (D2Q9, D3Q27).  No
+// reference counterpart (src/velocity_set.rs:168: D3Q27 has no collision): the
+// engine's definition, restated here for parity.  Central moments about u are
+// built axis by axis from the 3-point raw moments (M0 = f- + f0 + f+, M1 = f+ - f-,
+// M2 = f+ + f-; k0 = M0, k1 = M1 - u M0, k2 = M2 - 2 u M1 + u^2 M0); they relax
+// towards rho * c(a) c(b) c(c), c = (1, 0, 1/3): order 1 reflected, order 2
+// deviatoric and off-diagonal parts at 1/tau, the trace at rates[0], orders 3..6
+// at rates[1..4]; then the passes are inverted (M1 = k1 + u k0,
+// M2 = k2 + 2 u k1 + u^2 k0, f+ = (M2 + M1)/2, f- = (M2 - M1)/2, f0 = M0 - M2).
+void central(const VS& v, Float rho, const Float* u, const Float* f, const lbf_collision_desc& cd, Float* out) {
+    const int D = v.d;
+    Float k[27] = {};
+    auto pos = [&](int i) { return (v.c[i][0] + 1) + 3 * (v.c[i][1] + 1) + (D == 3 ? 9 * (v.c[i][2] + 1) : 0); };
+    for (int i = 0; i < v.q; ++i) k[pos(i)] = f[i];
+    const int nl = v.q / 3;
+    for (int a = 0; a < D; ++a) {
+        const int s = a == 0 ? 1 : (a == 1 ? 3 : 9);
+        for (int j = 0; j < nl; ++j) {
+            const int b = (j % s) + (j / s) * 3 * s;
+            const Float fm = k[b], f0 = k[b + s], fp = k[b + 2 * s];
+            const Float M0 = fm + f0 + fp, M1 = fp - fm, M2 = fp + fm;
+            k[b] = M0;
+            k[b + s] = M1 - u[a] * M0;
+            k[b + 2 * s] = M2 - 2.0 * u[a] * M1 + u[a] * u[a] * M0;
+        }
+    }
+    const Float om = 1.0 / cd.tau;
+    Float r[5];
+    for (int i = 0; i < 5; ++i) r[i] = cd.relaxation[i] > 0.0 ? cd.relaxation[i] : 1.0;
+    auto cf = [](int o) { return o == 0 ? 1.0 : (o == 1 ? 0.0 : 1.0 / 3.0); };
+    auto eq = [&](int a, int b, int c) { return rho * cf(a) * cf(b) * cf(c); };
+    // order 1
+    k[1] = -k[1];
+    k[3] = -k[3];
+    if (D == 3) k[9] = -k[9];
+    // order 2
+    if (D == 3) {
+        const Float dxx = k[2] - eq(2, 0, 0), dyy = k[6] - eq(0, 2, 0), dzz = k[18] - eq(0, 0, 2);
+        const Float tr = (1.0 - r[0]) * (dxx + dyy + dzz);
+        const Float dxy = (1.0 - om) * (dxx - dyy), dxz = (1.0 - om) * (dxx - dzz);
+        const Float nxx = (tr + dxy + dxz) / 3.0;
+        k[2] = eq(2, 0, 0) + nxx;
+        k[6] = eq(0, 2, 0) + (nxx - dxy);
+        k[18] = eq(0, 0, 2) + (nxx - dxz);
+        for (int p : {4, 10, 12}) k[p] = (1.0 - om) * k[p];
+    } else {
+        const Float dxx = k[2] - eq(2, 0, 0), dyy = k[6] - eq(0, 2, 0);
+        const Float tr = (1.0 - r[0]) * (dxx + dyy), dxy = (1.0 - om) * (dxx - dyy);
+        k[2] = eq(2, 0, 0) + 0.5 * (tr + dxy);
+        k[6] = eq(0, 2, 0) + 0.5 * (tr - dxy);
+        k[4] = (1.0 - om) * k[4];
+    }
+    // orders 3..6
+    for (int p = 0; p < v.q; ++p) {
+        const int a = p % 3, b = (p / 3) % 3, c = p / 9, ord = a + b + c;
+        if (ord < 3) continue;
+        const Float w = r[ord - 2];
+        const Float e = eq(a, b, c);
+        k[p] = e + (1.0 - w) * (k[p] - e);
+    }
+    for (int a = D - 1; a >= 0; --a) {
+        const int s = a == 0 ? 1 : (a == 1 ? 3 : 9);
+        for (int j = 0; j < nl; ++j) {
+            const int b = (j % s) + (j / s) * 3 * s;
+            const Float k0 = k[b], k1 = k[b + s], k2 = k[b + 2 * s];
+            const Float M1 = k1 + u[a] * k0, M2 = k2 + 2.0 * u[a] * k1 + u[a] * u[a] * k0;
+            k[b] = (M2 - M1) * 0.5;
+            k[b + s] = k0 - M2;
+            k[b + 2 * s] = (M2 + M1) * 0.5;
+        }
+    }
+    for (int i = 0; i < v.q; ++i) out[i] = k[pos(i)];
+}
+
 // Lattice::collision_step (src/momentum/lattice.rs:343-355)
 void m_collision(Domain& D) {
     const int64_t nf = (int64_t)D.fluid.size();
@@ -574,6 +648,8 @@ void m_collision(Domain& D) {
                     fs[i] += (1.0 - 0.5 * D.coll.omega_plus) * sp + (1.0 - 0.5 * D.coll.omega_minus) * sm;
                 }
             }
+        } else if (D.coll.kind == LBF_CENTRAL) {
+            central(v, D.rho[idx], u, f, D.coll, fs);
         } else {
             mrt(v, D.rho[idx], u, f, feq, D.coll.relaxation, D.compat, fs);
             if (D.has_force && D.compat == LBF_COMPAT_PHYSICS) {
@@ -979,6 +1055,14 @@ int orc_mrt(int id, double value, const double* u, const double* f, const double
             const double* relax, int compat, double* out) {
     VS v = make_vs(id); if (v.id < 0) return LBF_EUNSUPPORTED;
     mrt(v, value, u, f, feq, relax, compat, out); return LBF_OK;
+}
+int orc_central(int id, double rho, const double* u, const double* f, double tau, const double* rates5,
+                double* out) {
+    VS v = make_vs(id); if (v.id < 0 || (v.q != 9 && v.q != 27)) return LBF_EUNSUPPORTED;
+    lbf_collision_desc cd{};
+    cd.kind = LBF_CENTRAL; cd.tau = tau;
+    for (int i = 0; i < 5; ++i) cd.relaxation[i] = rates5[i];
+    central(v, rho, u, f, cd, out); return LBF_OK;
 }
 int orc_momentum_source(int id, const double* u, const double* F, double tau, double* out) {
     VS v = make_vs(id); if (v.id < 0) return LBF_EUNSUPPORTED;

@@ -43,6 +43,7 @@ def lib() -> C.CDLL:
         "orc_trt": (I32, [I32, PD, PD, D, D, PD]),
         "orc_mrt": (I32, [I32, D, PD, PD, PD, PD, I32, PD]),
         "orc_momentum_source": (I32, [I32, PD, PD, D, PD]),
+        "orc_central": (I32, [I32, D, PD, PD, D, PD, PD]),
         "orc_mrt_meq": (I32, [I32, D, PD, PD]),
         "orc_zou_he": (I32, [I32, I32, PD, I32, D, PI, PD]),
         "orc_create": (I32, [C.POINTER(_abi.DomainDesc), C.POINTER(P)]),
@@ -129,6 +130,14 @@ def mrt(vs, value, u, f, feq, relax, compat=0):
     u = np.ascontiguousarray(u, float); relax = np.ascontiguousarray(relax, float)
     out = np.zeros_like(f)
     _chk(lib().orc_mrt(vs, value, _pd(u), _pd(f), _pd(feq), _pd(relax), compat, _pd(out)))
+    return out
+
+
+def central(vs, rho, u, f, tau, rates=(1.0, 1.0, 1.0, 1.0, 1.0)):
+    """Central-moment collision of one node (rates: bulk, 3rd..6th order)."""
+    f = np.ascontiguousarray(f, float); u = np.ascontiguousarray(u, float)
+    r = np.ascontiguousarray(rates, float); out = np.zeros_like(f)
+    _chk(lib().orc_central(vs, rho, _pd(u), _pd(f), tau, _pd(r), _pd(out)))
     return out
 
 

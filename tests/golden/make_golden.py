@@ -6,7 +6,8 @@ src/velocity_set/*.rs and the expected values of the #[cfg(test)] functions in
 src/momentum/node.rs, src/momentum/lattice.rs, src/momentum/bc.rs,
 src/velocity_set.rs, src/velocity_set/d2q9.rs and src/velocity_set/d3q27.rs.
 
-Run from the repository root:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Run from the repository root:  python tests/golden/make_golden.py REFERENCE_ROOT
+(REFERENCE_ROOT: a checkout of the reference; required).
 The JSON it writes is committed; tests read only the JSON.
 """
 from __future__ import annotations
@@ -18,7 +19,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if __name__ == "__main__" and len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+REF = sys.argv[1] if len(sys.argv) > 1 else ""
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
 
 

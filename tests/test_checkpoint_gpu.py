@@ -67,3 +67,43 @@ def test_checkpoint_refuses_other_storage(Domain, tmp_path):
         with pytest.raises(_abi.LbfError) as ei:
             b.load(path)
         assert ei.value.status == _abi.LBF_EINVAL
+
+
+@pytest.mark.parametrize("damage", ["truncated", "section_count", "other_lattice"])
+def test_rejected_checkpoint_leaves_domain_unchanged(Domain, damage, tmp_path):
+    """A checkpoint that is refused (truncated, with a wrong section count, or of
+    another lattice) leaves the time step, the residuals and the fields as they
+    were, so that the next step reads the right population buffer."""
+    p = cases.cavity_d2q9(24, 0.6, 0.1, Storage.F32)
+    path = str(tmp_path / "state.ckpt")
+    with Domain(p) as a:
+        a.init().step(17, residual_interval=4)   # odd time step: the other buffer parity
+        a.save(path)
+    buf = np.fromfile(path, dtype=np.uint8)
+    if damage == "truncated":
+        buf = buf[: buf.size - 64]
+    elif damage == "section_count":
+        # CkptHeader: magic[8], vs q st d (4 x i32), N Np nlist (3 x i64), sparse scalar ads nsec (4 x i32)
+        off = 8 + 16 + 24 + 12
+        buf = buf.copy()
+        buf[off:off + 4] = np.frombuffer(np.int32(3).tobytes(), np.uint8)
+    else:
+        with Domain(cases.cavity_d2q9(20, 0.6, 0.1, Storage.F32)) as other:
+            other.init().step(5)
+            other.save(path)
+        buf = np.fromfile(path, dtype=np.uint8)
+    buf.tofile(path)
+    with Domain(p) as b, Domain(p) as ref:
+        b.init().step(10, residual_interval=4)
+        ref.init().step(10, residual_interval=4)
+        with pytest.raises(_abi.LbfError) as ei:
+            b.load(path)
+        assert ei.value.status == _abi.LBF_EINVAL
+        assert b.time_step == 10
+        assert np.array_equal(b.residuals()[0], ref.residuals()[0])
+        b.step(9, residual_interval=4)
+        ref.step(9, residual_interval=4)
+        rb, ub, _ = b.moments()
+        rr, ur, _ = ref.moments()
+        assert np.array_equal(rb, rr) and np.array_equal(ub, ur)
+        assert np.array_equal(b.residuals()[0], ref.residuals()[0])

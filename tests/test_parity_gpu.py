@@ -458,18 +458,3 @@ def test_sparse_layout_matches_oracle(Domain, name):
     assert rel(rg[fl], ro[fl]) <= TOL64 and rel(ug[fl], uo[fl]) <= TOL64
     assert t == steps - 1 and np.allclose(res, od.residuals(), rtol=1e-7, atol=1e-15)
     assert np.allclose(inv, od.inventory(), rtol=1e-12)
-
-
-@pytest.mark.parametrize("storage,tol", [(Storage.F16DEV, 3e-2), (Storage.BF16DEV, 2e-1)])
-def test_deviation_storage_bounded_error(Domain, storage, tol):
-    mask = cases.sphere_pack([24, 20, 16], 0.75, 2.0, 3.5, seed=11)
-    ref = cases.porous_channel_d3q19([24, 20, 16], mask=mask, force=1e-5, storage=Storage.F64)
-    low = cases.porous_channel_d3q19([24, 20, 16], mask=mask, force=1e-5, storage=storage)
-    with Domain(ref) as a, Domain(low) as b:
-        a.init().step(300)
-        b.init().step(300)
-        ra, ua, _ = a.moments()
-        rb, ub, _ = b.moments()
-    fl = mask == 0
-    assert rel(ub[fl], ua[fl]) <= tol
-    assert rel(rb[fl], ra[fl]) <= 1e-3

@@ -1,9 +1,9 @@
 """lbf_inventory_noalloc: the fluid-node FP64 sums without any device allocation.
 
 This entry point is for callers that cannot allocate device memory when they
-need the sums: code running inside a CUDA stream capture (allocation calls are
-not permitted there) or an application whose HBM is already reserved by its own
-allocator or by lattices sized to fill it.  The test prepares the input arrays
+need the sums: an application whose HBM is already reserved by its own caching
+allocator (an allocation behind its back breaks its accounting) or by lattices
+sized to fill it (an allocation would fail).  The test prepares the input arrays
 itself (with torch, as such a caller would have them), calls the entry point
 twice through the C ABI, and checks both results against lbf_domain_inventory,
 which computes the same sums with library-allocated scratch.  The file is named
