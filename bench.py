@@ -64,8 +64,9 @@ def parse():
     ap.add_argument("--sround", type=int, default=-1, help="16-bit storage: 1/0 stochastic rounding on/off")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the sweep variant and block size by timing candidates first (untimed)")
-    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy"],
+    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy", "c4"],
                     help="step: the fused step on one lattice (headline); serve: the serving mix; "
+                         "c4: the coupled momentum + scalar step on the packed bed (192x192x384); "
                          "batch: batched vs single-domain sweeps and per-request host costs; "
                          "accuracy: FP32 / FP16 / BF16 storage against FP64 at full size (--case)")
     ap.add_argument("--case", default="c2", choices=["c2", "c3", "c4"],
@@ -76,8 +77,12 @@ def parse():
                     help="accuracy c4: momentum collision (BGK tau 0.6 / 0.8, or TRT tau+ 0.8 / 0.55 magic 1/4)")
     ap.add_argument("--c4-u", type=float, default=0.01, help="accuracy c4: inlet velocity u_z")
     ap.add_argument("--c3-re", type=float, default=1600.0, help="accuracy c3: Reynolds number of the vortex")
-    ap.add_argument("--requests", type=int, default=300, help="serve: number of requests")
-    ap.add_argument("--rate", type=float, default=float("inf"), help="serve: Poisson arrivals per second (inf = all at t=0)")
+    ap.add_argument("--c3-collision", default="central", choices=["central", "mrt"],
+                    help="accuracy c3: central-moment collision (default) or the raw-moment MRT")
+    ap.add_argument("--requests", type=int, default=4000, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrivals per second (inf = all at t=0)")
+    ap.add_argument("--serve-mode", default="lanes", choices=["lanes", "single"],
+                    help="serve: two batches (small requests on a high-priority stream) or one batch")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
     ap.add_argument("--chunk", type=int, default=50, help="serve: residual interval (steps per chunk)")
     ap.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time baseline")
@@ -452,22 +457,122 @@ def run_engine(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_c4(args, rank, world, local_rank):
+    """The coupled D3Q19 momentum + passive-scalar step with Langmuir adsorption on
+    the packed bed (192 x 192 x 384, porosity 0.6 of seeded overlapping spheres
+    r in [4, 10], Zou-He inlet u_z = 0.04 with scalar C = 1, anti-bounce-back
+    outlet with second-order scalar outflow, scalar tau 0.55, k_a 1e-3, k_d 1e-5,
+    q_max 1; --c4-u and --c4-collision as in the accuracy run, whose defaults keep
+    the flow finite: at u_z = 0.04 the reference's algorithm diverges on this bed),
+    FP32 or FP64 storage: MFLUPS and the roofline of the step kernels.
+    Algorithmic bytes per fluid update: 2 Q s for f and 2 Q s for g, plus q_ads and
+    the previous scalar value read and written at each bounce-back node (4 s),
+    plus 1 B of node type per node."""
+    import torch
+    from lbflow_b200 import _abi, cases
+    from lbflow_b200.core import Storage
+    from lbflow_b200.domain import Domain
+    torch.cuda.set_device(local_rank)
+    st = {"f32": Storage.F32, "f64": Storage.F64}[args.storage if args.storage in ("f32", "f64") else "f32"]
+    side = 192 if args.n == 256 else args.n     # --n: a smaller bed of the same shape (n x n x 2n)
+    n = [side, side, 2 * side]
+    cache = os.path.join(tempfile.gettempdir(), "lbflow_b200_cache")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, f"bed_{side}x{side}x{2 * side}_{args.seed}_p060.npy")
+    if os.path.exists(path):
+        mask = np.load(path)
+    else:
+        mask = cases.sphere_pack(n, 0.6, 4.0, 10.0, args.seed, overlap=True)
+        np.save(path, mask)
+    # 8 clear layers at the inlet and the outlet, as in the accuracy run of this bed
+    mask = mask.reshape(n[2], n[1], n[0]).copy()
+    mask[:8] = 0
+    mask[-8:] = 0
+    mask = mask.ravel()
+    from lbflow_b200.core import BGK, TRT
+    coll = {"bgk0.6": BGK(0.6), "bgk0.8": BGK(0.8), "trt0.8": TRT.from_magic(0.8, 0.25),
+            "trt0.55": TRT.from_magic(0.55, 0.25)}[args.c4_collision]
+    mp, sp = cases.packed_bed_scalar(n, mask=mask, storage=st, u_in=args.c4_u, tau_g=0.55, collision=coll)
+    stream = torch.cuda.current_stream()
+    with Domain(mp, sp) as d:
+        configure(d, args, _abi)
+        d.init(stream)
+        cls, _ = d.node_class()
+        fl = (cls & _abi.LBF_CLASS_SOLID) == 0
+        n_fluid = int(np.count_nonzero(fl))
+        n_bb = int(np.count_nonzero(fl & ((cls & _abi.LBF_CLASS_BOUNCE_BACK) != 0)))
+        sweep = sweep_name(d, _abi)
+        with Clocks(local_rank) as clk:
+            ms = time_steps(d, args.steps, args.warmup, stream, world)
+        clocks = clk.summary()
+        inv = d.inventory()
+        finite = bool(np.all(np.isfinite(inv)))
+    sec = ms / 1e3
+    s_b = 8 if st == Storage.F64 else 4
+    alg = n_fluid * 4 * 19 * s_b + n_bb * 4 * s_b + mask.size
+    peak, kind = peaks()
+    achieved = alg / (sec / args.steps) / 1e9
+    if rank != 0:
+        return
+    line = {"metric": "MFLUPS", "value": world * n_fluid * args.steps / sec / 1e6, "unit": "MFLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if st == Storage.F64 else "f32",
+            "data": "synthetic (seeded sphere packing)",
+            "config": {"workload": "coupled D3Q19 momentum + D3Q19 scalar with Langmuir adsorption, packed bed "
+                                   f"{side}x{side}x{2 * side}, porosity 0.6 (8 clear layers at each end), Zou-He inlet "
+                                   f"u_z={args.c4_u:g}, momentum {args.c4_collision}, scalar tau 0.55",
+                       "storage": "f64" if st == Storage.F64 else "f32", "n_fluid": n_fluid,
+                       "bounce_back_nodes": n_bb, "sweep": sweep,
+                       "l2": "inputs larger than L2 (f and g populations, 2 buffers each)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": kind, "algorithmic_bytes_per_launch": alg},
+            "finite_after_run": finite, "gpu_launches": args.steps * 2, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args, rank, world, local_rank):
-    """The serving mix through one Batch, and one solve at a time as the baseline."""
+    """The serving mix through the batches, and one solve at a time as the baseline;
+    then the FP16-deviation requests of a sample are solved again in FP64 storage
+    and compared (velocity, relative L2), so that the batched results are shown to
+    be of the stated accuracy."""
+    import math
     import torch
     from lbflow_b200 import serve
+    from lbflow_b200.core import Storage
+    from lbflow_b200.domain import Domain
     torch.cuda.set_device(local_rank)
     reqs = serve.make_requests(args.requests, args.rate, args.seed + rank)
     serve.prepare(reqs)
     warm = serve.make_requests(6, float("inf"), args.seed + 999)
     serve.prepare(warm)
-    serve.serve_batched(warm, max_steps=200, residual_interval=args.chunk)
+    run = serve.serve_lanes if args.serve_mode == "lanes" else serve.serve_batched
+    run(warm, max_steps=200, residual_interval=args.chunk)
     serve.serve_sequential(warm, max_steps=200, residual_interval=args.chunk)
     torch.cuda.synchronize()
+    rng = np.random.default_rng(args.seed)
+    f16 = [r.rid for r in reqs if r.storage == Storage.F16DEV]
+    check = set(int(x) for x in rng.choice(f16, size=min(12, len(f16)), replace=False)) if f16 else set()
     with Clocks(local_rank) as clk:
-        rb = serve.serve_batched(reqs, max_steps=args.max_steps, residual_interval=args.chunk)
+        if args.serve_mode == "lanes":
+            rb = serve.serve_lanes(reqs, max_steps=args.max_steps, residual_interval=args.chunk, keep=check)
+        else:
+            rb = serve.serve_batched(reqs, max_steps=args.max_steps, residual_interval=args.chunk)
     sb = serve.summary(rb)
-    sb["host_times"] = getattr(serve.serve_batched, "host_times", None)
+    sb["host_times"] = getattr(run, "host_times", None)
+    # accuracy of the FP16 half: the same requests in FP64 storage, same stop rule
+    acc = []
+    fields = getattr(serve.serve_lanes, "fields", {}) if args.serve_mode == "lanes" else {}
+    for r in reqs:
+        if r.rid not in fields:
+            continue
+        p64 = serve.build_params(r)
+        p64.storage = Storage.F64
+        with Domain(p64) as d:
+            d.init().run(args.max_steps - 2, args.chunk, tol_density=math.inf, tol_velocity=1e-6, tol_scalar=math.inf)
+            _, u64, _ = d.moments()
+        u16 = fields[r.rid]
+        acc.append({"rid": r.rid, "kind": r.kind, "side": r.side,
+                    "rel_l2_velocity": float(np.linalg.norm(u16 - u64) / max(np.linalg.norm(u64), 1e-300))})
     ss = None
     if not args.no_sequential:
         ss = serve.summary(serve.serve_sequential(reqs, max_steps=args.max_steps, residual_interval=args.chunk))
@@ -491,8 +596,14 @@ def run_serve(args, rank, world, local_rank):
                                    "log-U[32,160] porosity U[0.5,0.9], FP32 / FP16-deviation storage 50/50, "
                                    f"stop at {args.max_steps} steps or velocity residual < 1e-6 "
                                    f"(checked every {args.chunk} steps)",
+                       "serving": ("two batches: small requests on a high-priority stream, smallest first; "
+                                   "large requests (>= 2^19 nodes) on a normal-priority stream")
+                       if args.serve_mode == "lanes" else "one batch",
                        "parallelism": "replicas" if world > 1 else "single"},
-            "batched": sb, "sequential": ss, "clocks": clk.summary()}
+            "p50_s": sb.get("p50_s"), "p99_s": sb.get("p99_s"),
+            "batched": sb, "sequential": ss, "fp16_vs_fp64": acc, "clocks": clk.summary()}
+    if acc:
+        line["fp16_vs_fp64_max_rel_l2_velocity"] = max(a["rel_l2_velocity"] for a in acc)
     if ss:
         line["speedup_vs_sequential"] = sb["solves_per_s"] / ss["solves_per_s"]
     if sp:
@@ -602,8 +713,9 @@ def run_accuracy(args, rank, world, local_rank):
     elif args.case == "c3":
         steps = args.acc_steps or 10000
         stores = [Storage.F64, Storage.F32, Storage.F16DEV]
-        mk = lambda st: cases.tgv_d3q27(384, 0.05, args.c3_re, st)[0]  # noqa: E731
+        mk = lambda st: cases.tgv_d3q27(384, 0.05, args.c3_re, st, collision=args.c3_collision)[0]  # noqa: E731
         out["c3_re"] = args.c3_re
+        out["c3_collision"] = args.c3_collision
         sample = list(range(0, steps + 1, 500))
     else:
         steps = args.acc_steps or 40000
@@ -778,6 +890,8 @@ def main():
         run_serve(args, rank, world, local_rank)
     elif args.workload == "batch":
         run_batch_probe(args, rank, world, local_rank)
+    elif args.workload == "c4":
+        run_c4(args, rank, world, local_rank)
     elif args.workload == "accuracy":
         run_accuracy(args, rank, world, local_rank)
     elif world > 1 and args.decomp == "slab":

@@ -240,15 +240,23 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  *                  buffer; an even step reads and writes each node's own slots, an
  *                  odd step its neighbours').  All three compute the same values bit
  *                  for bit; the in-place scheme needs half the population memory.
- *                  Default (-1): LBF_STREAM_PUSH; z-slabs always pull, and so do
+ *                  Default (-1): LBF_STREAM_PULL; z-slabs always pull, and so do
  *                  domains with explicit faces or a scalar.  Set before
  *                  lbf_domain_init.  get: the scheme in effect.
  * LBF_OPT_SROUND   16-bit deviation storage: 1 = stochastic rounding of the stored
  *                  values (seeded by node and time step, so runs repeat exactly),
  *                  0 = round to nearest; default 1.
+ * LBF_OPT_SEED_OFFSET  node index (in the whole lattice) of this lattice's node 0:
+ *                  a z-slab sets it so that its nodes round as in the whole lattice.
+ * LBF_OPT_WAIT_LIMIT  polls after which a bounded wait of the staged sweeps (on
+ *                  their bulk copies) gives up: the step then returns LBF_ETIMEOUT
+ *                  once the copies in flight have landed, and the domain stays
+ *                  usable (re-initialise it).  -1 = default (2^22 polls); 0 makes
+ *                  every such wait give up at once, to exercise that path.
  * lbf_domain_get_option reports whether STAGE / PIPE are in effect for the domain. */
 enum { LBF_OPT_BLOCK_X = 0, LBF_OPT_STAGE = 1, LBF_OPT_PIPE = 2, LBF_OPT_PIPE_STAGES = 3, LBF_OPT_COMPACT = 4,
-       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6, LBF_OPT_SPARSE = 7, LBF_OPT_STREAMING = 8, LBF_OPT_SROUND = 9 };
+       LBF_OPT_Z_BEGIN = 5, LBF_OPT_Z_END = 6, LBF_OPT_SPARSE = 7, LBF_OPT_STREAMING = 8, LBF_OPT_SROUND = 9,
+       LBF_OPT_WAIT_LIMIT = 10, LBF_OPT_SEED_OFFSET = 11 };
 enum { LBF_STREAM_PULL = 0, LBF_STREAM_PUSH = 1, LBF_STREAM_INPLACE = 2 };
 lbf_status lbf_domain_set_option(lbf_domain* dom, int32_t option, int64_t value);
 lbf_status lbf_domain_get_option(lbf_domain* dom, int32_t option, int64_t* value);

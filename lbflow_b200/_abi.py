@@ -25,7 +25,7 @@ LBF_STORE_F64, LBF_STORE_F32, LBF_STORE_F16DEV, LBF_STORE_BF16DEV = range(4)
 LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 
 (LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END,
- LBF_OPT_SPARSE, LBF_OPT_STREAMING, LBF_OPT_SROUND) = range(10)
+ LBF_OPT_SPARSE, LBF_OPT_STREAMING, LBF_OPT_SROUND, LBF_OPT_WAIT_LIMIT, LBF_OPT_SEED_OFFSET) = range(12)
 LBF_STREAM_PULL, LBF_STREAM_PUSH, LBF_STREAM_INPLACE = range(3)
 
 LBF_CLASS_SOLID = 0x1

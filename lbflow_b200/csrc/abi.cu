@@ -46,6 +46,18 @@ int vs_d(int vs) { return vs == LBF_D2Q9 ? 2 : 3; }
 size_t st_bytes(int st) { return st == LBF_STORE_F64 ? 8 : (st == LBF_STORE_F32 ? 4 : 2); }
 size_t rt_bytes(int st) { return st == LBF_STORE_F64 ? 8 : 4; }   // compute type
 
+// Residual and inventory partial sums: six accumulators, one slot per block of
+// the widest launch a domain can make (the dense sweep at 32 threads per block,
+// plus one face pass per face at 32 threads per block: an upper bound of every
+// other launch shape, 256-thread sparse and inventory sweeps included).
+constexpr int ACCUM_PLANES = 6;
+long long accum_slots(const long long* n, int nfaces) {
+    long long s = (n[0] + 31) / 32 * n[1] * n[2];
+    const long long N = n[0] * n[1] * n[2];
+    for (int f = 0; f < nfaces; ++f) s += (N / n[f / 2] + 31) / 32;
+    return s + 16;
+}
+
 // ---- device and pinned memory --------------------------------------------------
 // Serving creates and destroys domains continuously.  cudaMalloc / cudaFree (and
 // cudaFreeHost) synchronise the whole device and return memory to the driver
@@ -296,7 +308,9 @@ struct lbf_domain {
     void* qads = nullptr;
     void* cprev = nullptr;
     double* c_init_dev = nullptr;
-    double* accum = nullptr;
+    double* accum = nullptr;      // per-block partial sums: [accumulator][accum_cap]
+    long long accum_cap = 0;      // slots per accumulator (the most blocks any launch of the domain uses)
+    long long slot_next = 0;      // next free slot of the step being launched
     double* res_dev = nullptr;
     double* res_host = nullptr;   // pinned
     double* obs = nullptr;        // rho | u | c  (doubles)
@@ -323,6 +337,8 @@ struct lbf_domain {
     bool inplace = false;         // in effect: AA pattern, one population buffer (pop[0]); steps alternate even / odd
     bool push = false;            // in effect: push sweep (two buffers, the state is the post-stream field)
     int sround = 1;               // 16-bit storage: stochastic rounding
+    long long wait_limit = -1;    // LBF_OPT_WAIT_LIMIT: polls of the staged sweeps' bounded waits (-1 default)
+    long long seed_offset = 0;    // LBF_OPT_SEED_OFFSET: node index of node 0 in the whole lattice
     uint32_t* list = nullptr;     // work entries (fluid nodes + solid nodes sharing a sector)
     long long nlist = 0;
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
@@ -553,7 +569,7 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     const size_t eb = st_bytes(D->st);
     const bool lean = !D->facebc && !D->scalar;
     const bool whole = !z_restricted(D) && lean;
-    const int scheme = D->stream_opt < 0 ? LBF_STREAM_PUSH : D->stream_opt;
+    const int scheme = D->stream_opt < 0 ? LBF_STREAM_PULL : D->stream_opt;
     const bool inplace = whole && scheme == LBF_STREAM_INPLACE;
     D->push = whole && scheme == LBF_STREAM_PUSH;
     void* np[2] = {nullptr, nullptr};
@@ -685,6 +701,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.N = D->N;
     P.mask = D->mask;
     P.err = D->err;
+    P.wait_limit = D->wait_limit;
     P.list = D->list;
     P.nlist = D->nlist;
     P.kbeg = 0;
@@ -711,6 +728,7 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.sweep_mode = D->inplace ? ((t & 1) ? SWEEP_AA_ODD : SWEEP_AA_EVEN) : (D->push ? SWEEP_PUSH : SWEEP_PULL);
     P.sround = D->sround;
     P.tstep = (unsigned)t;
+    P.seed_offset = D->seed_offset;
     const lbf_collision_desc& c = D->desc.collision;
     P.coll = c.kind; P.compat = D->desc.compat; P.has_force = D->desc.has_force; P.first = t == 0;
     P.tau = c.tau;
@@ -732,6 +750,8 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
     P.mom_prev = D->mom[(t + 1) & 1];
     P.mom_cur = D->mom[t & 1];
     P.accum = D->accum;
+    P.accum_stride = D->accum_cap;
+    P.slot0 = 0;
     if (D->scalar) {
         const lbf_scalar_desc& s = D->sdesc;
         P.has_scalar = 1;
@@ -776,6 +796,15 @@ bool can_pipe(const lbf_domain* D) {
     if (z_restricted(D)) return false;
     const size_t rowb = D->n[0] * st_bytes(D->st);
     return !D->facebc && !D->scalar && rowb % 16 == 0 && 2 * D->q * rowb <= 200 * 1024;
+}
+
+// Every launch of a residual step writes its blocks' partial sums to its own
+// range of slots, from D->slot_next on (reset at the start of each step); the
+// finalize sums the D->slot_next slots the step filled.
+long long take_slots(lbf_domain* D, StepParams& P, long long blocks) {
+    P.slot0 = D->slot_next;
+    D->slot_next += blocks;
+    return blocks;
 }
 
 // Calls fn(IC<VS>, IC<COLL>) for the domain's velocity set and collision (the
@@ -835,45 +864,78 @@ cudaError_t launch_sparse_fs(lbf_domain* D, const StepParams& P, cudaStream_t s)
                                                                                  blocks, s);
         });
     };
-    cudaError_t e = one(P, (unsigned)((P.kend - P.kbeg + 255) / 256));
+    StepParams B = P;
+    const unsigned nb = (unsigned)((P.kend - P.kbeg + 255) / 256);
+    take_slots(D, B, nb);
+    cudaError_t e = one(B, nb);
     for (int f = 0; f < D->nfaces && e == cudaSuccess; ++f) {
         if (!(D->outflow >> f & 1u)) continue;
         StepParams F = P;
         F.face_pass = 1;
         F.fp_face = f;
-        e = one(F, (unsigned)((D->pb_plane[f] + 255) / 256));
+        const unsigned nf = (unsigned)((D->pb_plane[f] + 255) / 256);
+        take_slots(D, F, nf);
+        e = one(F, nf);
     }
     return e;
 }
 
 cudaError_t launch_sparse(lbf_domain* D, const StepParams& P, cudaStream_t s) {
     if (D->facebc || D->scalar) return launch_sparse_fs(D, P, s);
+    StepParams B = P;
+    take_slots(D, B, (P.kend - P.kbeg + 255) / 256);
     return by_kind(D, [&](auto V, auto C) {
-        return launch_step_sparse<decltype(V)::value, decltype(C)::value>(D->st, P, lam_of(D), s);
+        return launch_step_sparse<decltype(V)::value, decltype(C)::value>(D->st, B, lam_of(D), s);
     });
 }
 
 // The bulk sweep, then one face pass per scalar outflow face.
-cudaError_t launch_step_any(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+cudaError_t launch_step_any(lbf_domain* D, const StepParams& P0, cudaStream_t s) {
+    StepParams P = P0;
     if (D->sparse) return launch_sparse(D, P, s);
     const bool lean = !D->facebc && !D->scalar && !P.first && !P.observe && !P.face_pass;
-    if (D->pipe && lean && can_pipe(D)) {
+    // the persistent pipelined sweep is used on steps without residuals only
+    if (D->pipe && lean && !P.residual && can_pipe(D)) {
         cudaError_t e = launch_pipe(D, P, s);
         if (e != cudaErrorNotSupported) return e;
         cudaGetLastError();
     }
-    if (lean && D->compact && D->list) return launch_list(D, P, s);
+    if (lean && D->compact && D->list) {
+        take_slots(D, P, (D->nlist + 255) / 256);
+        return launch_list(D, P, s);
+    }
     const bool stage = D->stage && can_stage(D);
     const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
-    cudaError_t e = launch_one(D, P, stage, Launch{step_grid(D, b), b, s});
+    const dim3 g = step_grid(D, b);
+    take_slots(D, P, (long long)g.x * g.y * g.z);
+    cudaError_t e = launch_one(D, P, stage, Launch{g, b, s});
     for (int f = 0; f < D->nfaces && e == cudaSuccess; ++f) {
         if (!(D->outflow >> f & 1u)) continue;
         StepParams F = P;
         F.face_pass = 1;
         F.fp_face = f;
-        e = launch_one(D, F, false, Launch{dim3((unsigned)((D->pb_plane[f] + 127) / 128)), dim3(128), s});
+        const unsigned nb = (unsigned)((D->pb_plane[f] + 127) / 128);
+        take_slots(D, F, nb);
+        e = launch_one(D, F, false, Launch{dim3(nb), dim3(128), s});
     }
     return e;
+}
+
+// The slots a residual step (not the first step) of the whole lattice fills: the
+// same launch shapes as launch_step_any.
+long long residual_step_slots(const lbf_domain* D) {
+    long long faces = 0;
+    if (D->sparse) {
+        for (int f = 0; f < D->nfaces; ++f)
+            if (D->outflow >> f & 1u) faces += (D->pb_plane[f] + 255) / 256;
+        return (D->nlist + 255) / 256 + faces;
+    }
+    for (int f = 0; f < D->nfaces; ++f)
+        if (D->outflow >> f & 1u) faces += (D->pb_plane[f] + 127) / 128;
+    if (!D->facebc && !D->scalar && D->compact && D->list) return (D->nlist + 255) / 256;
+    const dim3 b = (D->stage && can_stage(D)) ? dim3((unsigned)D->n[0]) : step_block(D);
+    const dim3 g = step_grid(D, b);
+    return (long long)g.x * g.y * g.z + faces;
 }
 
 // Reads the device error flag after a synchronisation point.
@@ -944,7 +1006,7 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
         dev_free(tmp, D->dev);
     }
     if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("init kernel: ") + cudaGetErrorString(e));
-    CK(cudaMemsetAsync(D->accum, 0, NSLOT * NACC * sizeof(double), s));
+    CK(cudaMemsetAsync(D->err, 0, sizeof(int), s));   // a re-initialised domain starts without an error
     D->t = 0;
     D->res_step = -1;
     D->initialized = true;
@@ -963,10 +1025,11 @@ lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s
         base_params(D, P, t);
         P.residual = (k > 0 && t % k == 0) ? 1 : 0;
         P.write_mom = (k > 0 && (t % k == 0 || (t + 1) % k == 0)) ? 1 : 0;
+        D->slot_next = 0;
         cudaError_t e = launch_step_any(D, P, s);
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
         if (P.residual) {
-            k_finalize<<<1, 32, 0, s>>>(D->accum, 5, 1, D->res_dev);
+            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, 5, 1, D->res_dev);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(D->res_host, D->res_dev, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
             D->res_step = t;
@@ -985,6 +1048,7 @@ lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
     StepParams P;
     base_params(D, P, D->t);
     P.observe = 1;
+    D->slot_next = 0;
     P.obs_rho = D->obs;
     P.obs_u = D->obs + D->N;
     P.obs_c = D->obs + D->N * (1 + D->d);
@@ -1005,6 +1069,7 @@ cudaError_t sweep_planes(lbf_domain* D, StepParams P, long long zlo, long long z
     const bool stage = D->stage && can_stage(D);
     const dim3 b = stage ? dim3((unsigned)D->n[0]) : step_block(D);
     const dim3 g((unsigned)((D->n[0] + b.x - 1) / b.x), (unsigned)D->n[1], (unsigned)(zhi - zlo));
+    take_slots(D, P, (long long)g.x * g.y * g.z);
     return launch_one(D, P, stage, Launch{g, b, s});
 }
 
@@ -1202,13 +1267,17 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     const size_t pbytes = (size_t)D->q * D->Np * st_bytes(D->st);
     for (int k = 0; k < 2; ++k)
         if ((st = dmalloc(D, &D->pop[k], pbytes))) { delete D; return st; }
-    if ((st = dmalloc(D, (void**)&D->accum, NSLOT * NACC * sizeof(double)))) { delete D; return st; }
+    D->accum_cap = accum_slots(n, nf);
+    if ((st = dmalloc(D, (void**)&D->accum, (size_t)ACCUM_PLANES * D->accum_cap * sizeof(double)))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->res_dev, 8 * sizeof(double)))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->err, sizeof(int)))) { delete D; return st; }
     if (cudaMemset(D->err, 0, sizeof(int)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
     if (!(D->res_host = (double*)pinned64())) { delete D; return fail(LBF_ENOMEM, "pinned alloc"); }
     std::memset(D->res_host, 0, 8 * sizeof(double));
-    if (cudaMemset(D->accum, 0, NSLOT * NACC * sizeof(double)) != cudaSuccess) { delete D; return fail(LBF_EDEVICE, "memset"); }
+    if (cudaMemset(D->accum, 0, (size_t)ACCUM_PLANES * D->accum_cap * sizeof(double)) != cudaSuccess) {
+        delete D;
+        return fail(LBF_EDEVICE, "memset");
+    }
     *out = D;
     return LBF_OK;
 }
@@ -1290,6 +1359,7 @@ lbf_status lbf_domain_step_part(lbf_domain* D, int32_t part, int64_t k, void* st
     P.write_mom = (k > 0 && (t % k == 0 || (t + 1) % k == 0)) ? 1 : 0;
     cudaError_t e = cudaSuccess;
     if (part == 0) {
+        D->slot_next = 0;   // the slots of both parts of the step
         e = sweep_planes(D, P, z0, z0 + 1, s);
         if (e == cudaSuccess && z1 - 1 > z0) e = sweep_planes(D, P, z1 - 1, z1, s);
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
@@ -1298,7 +1368,7 @@ lbf_status lbf_domain_step_part(lbf_domain* D, int32_t part, int64_t k, void* st
         e = sweep_planes(D, P, z0 + 1, z1 - 1, s);
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
         if (P.residual) {
-            k_finalize<<<1, 32, 0, s>>>(D->accum, 5, 1, D->res_dev);
+            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, 5, 1, D->res_dev);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(D->res_host, D->res_dev, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
             D->res_step = t;
@@ -1410,16 +1480,16 @@ lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     const double* uu = D->obs + N + o * D->d;
     const double* cc = c ? c + o : nullptr;
     if (D->d == 2) {
-        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum);
-        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum);
+        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum, D->accum_cap);
+        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum, D->accum_cap);
     } else {
-        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum);
-        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum);
+        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum, D->accum_cap);
+        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum, D->accum_cap);
     }
     CK(cudaGetLastError());
     double* tmp = nullptr;
     CK(dev_alloc((void**)&tmp, 8 * sizeof(double), D->dev));
-    k_finalize<<<1, 32, 0, s>>>(D->accum, 6, 0, tmp);
+    k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, (long long)nb, 6, 0, tmp);
     double h[8];
     cudaError_t e = cudaMemcpyAsync(h, tmp, 8 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1479,6 +1549,13 @@ lbf_status lbf_domain_set_option(lbf_domain* D, int32_t option, int64_t value) {
         case LBF_OPT_SROUND:
             D->sround = value != 0 ? 1 : 0;
             return LBF_OK;
+        case LBF_OPT_WAIT_LIMIT:
+            if (value < -1) return fail(LBF_EINVAL, "wait limit: -1 (default) or a number of polls >= 0");
+            D->wait_limit = value;
+            return LBF_OK;
+        case LBF_OPT_SEED_OFFSET:
+            D->seed_offset = value;
+            return LBF_OK;
         case LBF_OPT_Z_BEGIN:
         case LBF_OPT_Z_END:
             if (D->prepared) return fail(LBF_ESTATE, "set the swept z planes before lbf_domain_init");
@@ -1505,6 +1582,8 @@ lbf_status lbf_domain_get_option(lbf_domain* D, int32_t option, int64_t* value) 
             *value = D->inplace ? LBF_STREAM_INPLACE : (D->push ? LBF_STREAM_PUSH : LBF_STREAM_PULL);
             return LBF_OK;
         case LBF_OPT_SROUND: *value = D->sround; return LBF_OK;
+        case LBF_OPT_WAIT_LIMIT: *value = D->wait_limit; return LBF_OK;
+        case LBF_OPT_SEED_OFFSET: *value = D->seed_offset; return LBF_OK;
         case LBF_OPT_Z_BEGIN: *value = zb(D); return LBF_OK;
         case LBF_OPT_Z_END: *value = ze(D); return LBF_OK;
         default: return fail(LBF_EINVAL, "unknown option");
@@ -1737,10 +1816,11 @@ size_t kparams_size(int vs) {
 }
 
 // The domain's step parameters laid out for an even time step (t = 0 layout).
-void fill_kparams(const lbf_domain* D, unsigned char* dst) {
+void fill_kparams(const lbf_domain* D, unsigned char* dst, long long res_slots) {
     StepParams P;
     base_params(D, P, 0);
     P.first = 0;
+    P.res_slots = res_slots;
     if (D->vs == LBF_D3Q27) {
         KParams<VS_D3Q27>* kp = new KParams<VS_D3Q27>();
         static_cast<StepParams&>(*kp) = P;
@@ -1885,7 +1965,9 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         for (size_t p = 0; p < n; ++p) {
             const lbf_batch::Member& m = b->members[g.mem[p]];
             const lbf_domain* D = m.D;
-            fill_kparams(D, tab.data() + p * ks);
+            const long long units = D->sparse ? D->nlist : D->N;   // fluid nodes, or all nodes
+            const long long nb = g.solo ? 0 : (units + BATCH_BLOCK - 1) / BATCH_BLOCK;
+            fill_kparams(D, tab.data() + p * ks, g.solo ? residual_step_slots(D) : nb);
             BatchState& x = bs[p];
             std::memset(&x, 0, sizeof(x));
             x.t0 = D->t;
@@ -1898,8 +1980,6 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
             x.d = D->d;
             x.has_scalar = D->scalar ? 1 : 0;
             for (int i = 0; i < 3; ++i) x.tol[i] = m.tol[i];
-            const long long units = D->sparse ? D->nlist : D->N;   // fluid nodes, or all nodes
-            const long long nb = g.solo ? 0 : (units + BATCH_BLOCK - 1) / BATCH_BLOCK;
             blk.insert(blk.end(), (size_t)nb, (int)p);
         }
         if (blk.size() >= (1ull << 31)) return fail(LBF_EUNSUPPORTED, "batch group larger than 2^31 blocks");
@@ -1942,6 +2022,7 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
                 P.write_mom = (t % b->k == 0 || (t + 1) % b->k == 0) ? 1 : 0;
                 P.gate = (const GateView*)g.bs;
                 P.gate_j = j;
+                D->slot_next = 0;   // the step's partial-sum slots start at 0
                 e = launch_step_any(D, P, sg);
             }
             if (e == cudaSuccess) e = batch_launch_finalize(g, sg);
@@ -1983,7 +2064,10 @@ long long estimate_bytes(const lbf_domain_desc* ds, const lbf_scalar_desc* sd) {
     const long long plane = N / std::min({ds->n[0], ds->n[1], d == 3 ? ds->n[2] : ds->n[1]});
     b += 6 * 2 * 2 * (d + 1) * plane * rb;               // face layers (upper bound)
     if (sd) b += 6 * 2 * q * plane * rb;                 // outflow snapshots (upper bound)
-    b += NSLOT * NACC * 8 + 4096;
+    {
+        const long long nn[3] = {ds->n[0], ds->n[1], d == 3 ? ds->n[2] : 1};
+        b += ACCUM_PLANES * accum_slots(nn, d == 2 ? 4 : 6) * 8 + 4096;
+    }
     return b;
 }
 

@@ -250,24 +250,33 @@ static __global__ void k_fill_solid(const uint8_t* type, long long N, int d, dou
     if (c) c[i] = c0;
 }
 
-// Sum the NSLOT partials of each accumulator; out[k] = sqrt(sum) for residuals
-// or the plain sum for inventories; clears the partials for the next use.
-static __global__ void k_finalize(double* accum, int nacc, int take_sqrt, double* out) {
-    const int k = threadIdx.x;
-    if (k >= nacc) return;
-    double s = 0.0;
-    for (int j = 0; j < NSLOT; ++j) {
-        s += accum[j * NACC + k];
-        accum[j * NACC + k] = 0.0;
+// Sum the per-block partials (slots [0, nslots) of each of nacc accumulators,
+// accum[k * stride + slot]) in a fixed order: thread t adds slots t, t + T, ...
+// in turn, then a fixed tree adds the threads' sums.  out[k] = sqrt(sum) for
+// residuals, the plain sum for inventories.  One block of FINALIZE_THREADS.
+constexpr int FINALIZE_THREADS = 512;
+static __global__ void k_finalize(const double* accum, long long stride, long long nslots, int nacc, int take_sqrt,
+                                  double* out) {
+    __shared__ double part[FINALIZE_THREADS];
+    for (int k = 0; k < nacc; ++k) {
+        double s = 0.0;
+        for (long long j = threadIdx.x; j < nslots; j += FINALIZE_THREADS) s += accum[k * stride + j];
+        part[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = FINALIZE_THREADS / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[k] = take_sqrt ? sqrt(part[0]) : part[0];
+        __syncthreads();
     }
-    out[k] = take_sqrt ? sqrt(s) : s;
 }
 
 // FP64 inventories over fluid nodes from observed moments:
 // [sum rho, sum rho*u_a (D), sum C, sum q_ads].
 template <int D, class R>
 __global__ void k_inventory(const uint32_t* mask, long long N, const double* rho, const double* u, const double* c,
-                            const R* qads, double* accum) {
+                            const R* qads, double* accum, long long stride) {
     const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     double vq = 0.0;
@@ -279,7 +288,7 @@ __global__ void k_inventory(const uint32_t* mask, long long N, const double* rho
     }
     if (D == 2) v[4] = vq;   // slots: rho, j0, j1, C, q   (2-D)
     double w[6] = {v[0], v[1], v[2], v[3], v[4], D == 3 ? vq : 0.0};
-    block_accumulate<6>(w, accum);
+    block_partials<6>(w, accum, stride, blockIdx.x);
 }
 
 }  // namespace lbf

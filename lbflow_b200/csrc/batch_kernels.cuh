@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
         const unsigned grp = (per >= 32 ? 0xffffffffu : ((1u << per) - 1u) << ((lane / per) * per));
         if (inside && (mk & M_SOLID) && (fl & grp)) sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
     }
-    if (P.residual) block_accumulate<5>(racc, P.accum);
+    if (P.residual) step_partials<5>(racc, P, blockIdx.x - bs[e].block0);
 }
 
 // The batched sweep over domains in the sparse (fluid-only) layout: block b
@@ -148,10 +148,10 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
     else if (Ps.sweep_mode == SWEEP_AA_ODD) sparse_node<VS, COLL, ST, SWEEP_AA_ODD>(Ps, k, racc);
     else if (Ps.sweep_mode == SWEEP_PUSH) sparse_node<VS, COLL, ST, SWEEP_PUSH>(Ps, k, racc);
     else sparse_node<VS, COLL, ST, SWEEP_PULL>(Ps, k, racc);
-    if (Ps.residual) block_accumulate<5>(racc, Ps.accum);
+    if (Ps.residual) step_partials<5>(racc, Ps, blockIdx.x - bs[e].block0);
 }
 
-// One block of 32 threads per domain: residuals of the chunk's last step (its
+// One block of 256 threads per domain: residuals of the chunk's last step (its
 // residual step), the stop rule of lbf_domain_run, and t0 += k.
 template <int VS>
 __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState* __restrict__ bs, int n) {
@@ -162,19 +162,24 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
     const int k = s.k;
     const long long t_end = s.t0 + k - 1;
     const bool ran = t_end <= s.last_t;
-    double* accum = tab[e].accum;
+    const double* accum = tab[e].accum;
+    const long long stride = tab[e].accum_stride, nslots = tab[e].res_slots;
     __shared__ double r[8];
-    const int a = threadIdx.x;
-    if (a < 5) {
+    __shared__ double part[256];
+    // the per-block partials of the residual step, summed in slot order
+    for (int a = 0; a < 5; ++a) {
         double sum = 0.0;
-        for (int jj = 0; jj < NSLOT; ++jj) {
-            sum += accum[jj * NACC + a];
-            accum[jj * NACC + a] = 0.0;
+        for (long long jj = threadIdx.x; jj < nslots; jj += blockDim.x) sum += accum[a * stride + jj];
+        part[threadIdx.x] = sum;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+            __syncthreads();
         }
-        r[a] = sqrt(sum);
+        if (threadIdx.x == 0) r[a] = sqrt(part[0]);
+        __syncthreads();
     }
-    __syncthreads();
-    if (a == 0) {
+    if (threadIdx.x == 0) {
         if (ran) {
             for (int i = 0; i < 5; ++i) s.res[i] = r[i];
             s.res_t = t_end;
@@ -226,7 +231,7 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
     template <>                                                                                    \
     cudaError_t launch_batch_finalize<VS_>(const void* tab, BatchState* bs, int n, cudaStream_t s) { \
         if (n == 0) return cudaSuccess;                                                            \
-        k_batch_finalize<VS_><<<n, 32, 0, s>>>((const KParams<VS_>*)tab, bs, n);                   \
+        k_batch_finalize<VS_><<<n, 256, 0, s>>>((const KParams<VS_>*)tab, bs, n);                  \
         return cudaGetLastError();                                                                 \
     }
 

@@ -94,6 +94,7 @@ struct StepParams {
     int observe, write_mom, residual;
     int face_pass, fp_face;   // face pass: update the nodes of face fp_face only
     int* err;                 // set to 1 when a bounded wait gives up
+    long long wait_limit;     // polls of a bounded wait before it gives up (< 0: WAIT_LIMIT)
     int pipe_stages, pipe_nc; // pipelined sweep: ring stages, consumer warps
     const uint32_t* list;     // compacted sweep: work entries (see k_step_list)
     long long nlist;
@@ -114,6 +115,7 @@ struct StepParams {
     int sround;               // 16-bit storage: 1 = stochastic rounding (seeded by node and time step), 0 = nearest
     unsigned tstep;           // time step of the launch (low 32 bits; the rounding seed)
     int tpad;
+    long long seed_offset;    // node index of this lattice's node 0 in the whole lattice (z-slabs)
     double bgk_cb, s_bgk_cb;  // 1 - 1/(2 tau) of the momentum and scalar BGK sources, computed once
     // post-stream scalar populations of layers 1 and 2 inside each outflow face,
     // written by the bulk sweep and read by the face pass of the same step:
@@ -127,7 +129,9 @@ struct StepParams {
     // per-node moments for residuals: [field][N] (rho, u_0.., C), compute type
     const void* mom_prev;
     void* mom_cur;
-    double* accum;   // [NSLOT][NACC]
+    double* accum;   // residual partials: [accumulator][accum_stride] per-block slots
+    long long accum_stride, slot0;   // slots per accumulator; first slot of this launch's blocks
+    long long res_slots;             // batches: slots a member's residual step fills
     double* obs_rho;
     double* obs_u;
     double* obs_c;
@@ -279,6 +283,46 @@ __device__ __forceinline__ long long face_pos(const Geo& g, int f, const StepPar
 }
 
 // ---- reductions ----------------------------------------------------------------
+// Per-block partial sums: the block whose slot is `slot` writes its K sums to
+// accum[k * stride + slot].  No two blocks share an address and k_finalize adds
+// the slots in index order, so a sum does not depend on how the blocks were
+// scheduled: residuals, inventories and the steps at which a run stops repeat
+// bit for bit from run to run.
+template <int K>
+__device__ __forceinline__ void block_partials(double (&v)[K], double* accum, long long stride, long long slot) {
+    __shared__ double red[32][K];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) red[wid][k] = s;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = lane < nw ? red[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) accum[k * stride + slot] = s;
+        }
+    }
+}
+// The linear index of this block within its launch.
+__device__ __forceinline__ long long block_linear() {
+    return blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+}
+template <int K>
+__device__ __forceinline__ void step_partials(double (&v)[K], const StepParams& P, long long local_block) {
+    block_partials<K>(v, P.accum, P.accum_stride, P.slot0 + local_block);
+}
+
+// Partial sums into NSLOT shared slots with atomics: for a caller-provided
+// scratch of fixed size (the allocation-free entry point); the order of the
+// additions within a slot is not fixed.
 template <int K>
 __device__ __forceinline__ void block_accumulate(double (&v)[K], double* accum) {
     __shared__ double red[32][K];
@@ -814,8 +858,8 @@ __host__ __device__ constexpr int cm_pos(int i) {
 
 template <int VS, int ST, class StoreFn>
 __device__ __forceinline__ void central_collide(const KParams<VS>& P, typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                                typename Store<ST>::R rho, const typename Store<ST>::R* u,
-                                                StoreFn&& store) {
+                                                typename Store<ST>::R rho, typename Store<ST>::R drho,
+                                                const typename Store<ST>::R* u, StoreFn&& store) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
@@ -841,14 +885,26 @@ __device__ __forceinline__ void central_collide(const KParams<VS>& P, typename S
     // relaxation; k(a, b, c) sits at a + 3 b + 9 c (a, b, c = moment order per axis)
     const R om = R(P.omega), ob = R(P.rates[0]);
     const R w3 = R(P.rates[1]), w4 = R(P.rates[2]), w5 = R(P.rates[3]), w6 = R(P.rates[4]);
-    auto mfac = [&](int a, int ax) -> R {   // weights' central moment factor along axis ax
-        return a == 0 ? R(1) : (a == 1 ? -u[ax] : R(1.0 / 3.0) + u[ax] * u[ax]);
-    };
-    auto eq = [&](int a, int b, int c) -> R {   // equilibrium target (minus the weights' part)
-        auto cf = [](int o) { return o == 0 ? 1.0 : (o == 1 ? 0.0 : 1.0 / 3.0); };
-        R e = rho * R(cf(a) * cf(b) * cf(c));
-        if constexpr (DEV) e -= mfac(a, 0) * mfac(b, 1) * (D == 3 ? mfac(c, 2) : R(1));
-        return e;
+    // Equilibrium targets.  Without deviations: rho * c(a) c(b) c(c).  With
+    // deviations, minus the weights' central moments m(a) m(b) m(c), where
+    // m = c + d with d(0) = 0, d(1) = -u, d(2) = u^2; the difference
+    // rho c(a)c(b)c(c) - m(a)m(b)m(c) = drho * c(a)c(b)c(c) - Delta is evaluated as
+    // Delta_1 = d_1, Delta_k = Delta_{k-1} (c_k + d_k) + (c_1 .. c_{k-1}) d_k, so that
+    // no O(1) terms cancel (rho itself is 1 + drho and would lose drho's low bits).
+    auto cf = [](int o) -> R { return o == 0 ? R(1) : (o == 1 ? R(0) : R(1.0 / 3.0)); };
+    auto df = [&](int o, int ax) -> R { return o == 0 ? R(0) : (o == 1 ? -u[ax] : u[ax] * u[ax]); };
+    auto eq = [&](int a, int b, int c) -> R {
+        if constexpr (DEV) {
+            const int o[3] = {a, b, c};
+            R delta = df(a, 0), cprod = cf(a);
+            for (int ax = 1; ax < D; ++ax) {
+                delta = delta * (cf(o[ax]) + df(o[ax], ax)) + cprod * df(o[ax], ax);
+                cprod = cprod * cf(o[ax]);
+            }
+            return drho * cprod - delta;
+        } else {
+            return rho * cf(a) * cf(b) * (D == 3 ? cf(c) : R(1));
+        }
     };
     // first order: reflection about the equilibrium value (-u with deviations, 0 otherwise)
     sfor<D>([&](auto A) {
@@ -1010,7 +1066,7 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
             }
         });
     } else if constexpr (COLL == COLL_CENTRAL) {
-        if constexpr (L::Q == 9 || L::Q == 27) central_collide<VS, ST>(P, f, rho, u, store);
+        if constexpr (L::Q == 9 || L::Q == 27) central_collide<VS, ST>(P, f, rho, dr, u, store);
     } else if constexpr (VS == VS_D3Q27) {
         // population-space MRT, f* = f - Lambda (f - f_eq) (+ the Guo source in physics
         // mode): only the Q deviations e = f - f_eq (+ s/2) stay live through the
@@ -1085,6 +1141,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned phase,
     return false;
 }
 constexpr long long WAIT_LIMIT = 1ll << 22;
+// The limit of a step's waits on its copies; the waits that let copies in flight
+// land before a block exits always use WAIT_LIMIT.
+__device__ __forceinline__ long long wait_limit(const StepParams& P) {
+    return P.wait_limit < 0 ? WAIT_LIMIT : P.wait_limit;
+}
 
 
 // A launch that belongs to a stopped batch member, or to a step past its last
@@ -1200,7 +1261,11 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
         // ---- equilibrium + collision --------------------------------------------
         R uu = R(0);
         sfor<D>([&](auto A) { uu += u[A] * u[A]; });
-        const uint32_t nseed = (ST == ST_F16 || ST == ST_BF16) ? mix32((uint32_t)g.slot ^ (P.tstep * 0x9e3779b9u)) : 0u;
+        // the seed follows the node (index in the whole lattice), so every layout,
+        // streaming scheme and z-slab split rounds a node's values alike
+        const uint32_t nseed = (ST == ST_F16 || ST == ST_BF16)
+                                   ? mix32((uint32_t)((long long)g.cell + P.seed_offset) ^ (P.tstep * 0x9e3779b9u))
+                                   : 0u;
         collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, nseed, put);
 
         if constexpr (SCALAR) {
@@ -1331,7 +1396,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
                     if constexpr (SCALAR) bulk_g2s(grows + (size_t)i * P.nx, (const R*)P.gsrcp[i] + row, grb, bar);
                 });
             }
-            if (!mbar_wait_bounded(bar, 0, WAIT_LIMIT)) {
+            if (!mbar_wait_bounded(bar, 0, wait_limit(P))) {
                 if (threadIdx.x == 0 && P.err) atomicExch(P.err, 1);
                 mbar_wait_bounded(bar, 0, WAIT_LIMIT);   // let the copies in flight land
                 return;
@@ -1419,7 +1484,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
             if constexpr (SCALAR) sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = R(0); });
         }
     }
-    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+    if (P.residual && !P.observe) step_partials<5>(racc, P, block_linear());
 }
 
 // =================================================================== compacted sweep
@@ -1497,7 +1562,7 @@ __global__ void __launch_bounds__(256, ST == ST_F64 ? 2 : 4) k_step_list(const K
     } else if (valid) {
         sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
     }
-    if (P.residual) block_accumulate<5>(racc, P.accum);
+    if (P.residual) step_partials<5>(racc, P, blockIdx.x);
 }
 
 // Marks the work entries of the compacted sweep and encodes them (see k_step_list).
@@ -1558,7 +1623,7 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
             for (long long r = blockIdx.x; r < nrows; r += gridDim.x, ++k) {
                 const int s = (int)(k % NS);
                 const long long use = k / NS;
-                if (use > 0 && !mbar_wait_bounded(&empty[s], (unsigned)((use - 1) & 1), WAIT_LIMIT)) {
+                if (use > 0 && !mbar_wait_bounded(&empty[s], (unsigned)((use - 1) & 1), wait_limit(P))) {
                     failed = true;
                     break;
                 }
@@ -1586,7 +1651,7 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
         for (long long r = blockIdx.x; r < nrows; r += gridDim.x, ++k) {
             const int s = (int)(k % NS);
             const long long use = k / NS;
-            if (!mbar_wait_bounded(&full[s], (unsigned)(use & 1), WAIT_LIMIT)) {
+            if (!mbar_wait_bounded(&full[s], (unsigned)(use & 1), wait_limit(P))) {
                 if (lane == 0 && P.err) atomicExch(P.err, 1);
                 break;
             }
@@ -1638,7 +1703,7 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
             if (lane == 0) mbar_arrive(&empty[s]);
         }
     }
-    if (P.residual) block_accumulate<5>(racc, P.accum);
+    if (P.residual) step_partials<5>(racc, P, blockIdx.x);
 }
 
 // =================================================================== sparse sweep
@@ -1732,7 +1797,8 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
     const bool valid = k64 < P.nlist;
     const int k = valid ? (int)k64 : (int)(P.nlist - 1);
     // an in-place even step reads the node's own slots: coordinates only for outputs
-    const bool need_geo = MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom;
+    constexpr bool SIXTEEN = ST == ST_F16 || ST == ST_BF16;
+    const bool need_geo = MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom || (SIXTEEN && P.sround);
     Geo g;
     g.x = g.y = g.z = g.cell = 0;
     g.slot = k;
@@ -1881,22 +1947,25 @@ __device__ __forceinline__ void sparse_prefetch(const KParams<VS>& P) {
     }
 }
 
-// An in-place odd step keeps the Q slot offsets of its loads for its stores: 80
-// registers (three blocks per SM) instead of the 64 of the other light sweeps.
+// Blocks per SM of the sparse sweeps: 64 registers for the light ones.  (An
+// in-place odd step, which keeps the Q slot offsets of its loads for its stores,
+// spills 36 B at 64 registers; at 80 registers, three blocks per SM, it measured
+// 520 us per launch on the 256^3 headline lattice against 450 us with the spill.)
 template <int VS, int COLL, int ST, int MODE>
 constexpr int sparse_blocks() {
-    return light_kernel<VS, COLL, ST, false>() == 2 ? (MODE == SWEEP_AA_ODD ? 3 : 4) : 2;
+    return light_kernel<VS, COLL, ST, false>() == 2 ? 4 : 2;
 }
 
 template <int VS, int COLL, int ST, int MODE>
 __global__ void __launch_bounds__(256, (sparse_blocks<VS, COLL, ST, MODE>())) k_step_sparse(const KParams<VS> P) {
     if (gated_off(P)) return;
     // an in-place even step reads only its own contiguous slots: nothing to prefetch
-    if (MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom) sparse_prefetch<VS, ST>(P);
+    if (MODE != SWEEP_AA_EVEN || P.observe || P.residual || P.write_mom || ((ST == ST_F16 || ST == ST_BF16) && P.sround))
+        sparse_prefetch<VS, ST>(P);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const long long k = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
     sparse_node<VS, COLL, ST, MODE>(P, k < P.kend ? k : P.nlist, racc);   // nlist: no update
-    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+    if (P.residual && !P.observe) step_partials<5>(racc, P, blockIdx.x);
 }
 
 // =================================================================== sparse sweep, faces and scalar
@@ -2012,7 +2081,7 @@ __global__ void __launch_bounds__(256, 2) k_step_sparse_fs(const KParams<VS> P) 
         process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc,
                                                         [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[k] = v; });
     }
-    if (P.residual && !P.observe) block_accumulate<5>(racc, P.accum);
+    if (P.residual && !P.observe) step_partials<5>(racc, P, blockIdx.x);
 }
 
 // =================================================================== z-slab halos

@@ -9,9 +9,10 @@ Requests (the serving mix): Poisson arrivals at rate `rate` per second; half
 residual drops below `tol_velocity` (checked every `residual_interval` steps,
 with the rule of `Domain.run`).  Everything is generated from one seed.
 
-`serve_batched` runs the requests through one `Batch`; `serve_sequential` runs
-them one at a time with `Domain.run` in arrival order (the same stop rule, so the
-same fields and step counts).  Both record per request the arrival, start and
+`serve_batched` runs the requests through one `Batch`; `serve_lanes` through two
+batches that advance independently (small requests on a high-priority stream,
+smallest first); `serve_sequential` runs them one at a time with `Domain.run` in
+arrival order (the same stop rule, so the same fields and step counts).  Both record per request the arrival, start and
 finish times (finish = after the density and velocity fields reached the host).
 """
 from __future__ import annotations
@@ -187,6 +188,154 @@ def serve_batched(reqs: List[Request], max_steps: int = 2000, tol_velocity: floa
         host["moments_tail_s"] = time.perf_counter() - t1
         pool.shutdown(wait=True)
     serve_batched.host_times = host
+    return records
+
+
+def request_nodes(r: Request) -> int:
+    return int(r.side) ** (2 if r.kind == "cavity" else 3)
+
+
+def lane_of(r: Request, large_nodes: int) -> int:
+    """0: the small-request lane, 1: the large-request lane."""
+    return 1 if request_nodes(r) >= large_nodes else 0
+
+
+class _Arrivals:
+    """Requests that have arrived and wait to be built, smallest work first
+    (nodes x steps is the same step budget for all, so nodes decide)."""
+
+    def __init__(self, reqs: List[Request]):
+        import heapq
+        self._heapq = heapq
+        self.pending = sorted(reqs, key=lambda r: r.arrival)
+        self.i = 0
+        self.heap: list = []
+
+    def arrive(self, now: float) -> None:
+        while self.i < len(self.pending) and self.pending[self.i].arrival <= now:
+            r = self.pending[self.i]
+            self._heapq.heappush(self.heap, (request_nodes(r), r.rid, r))
+            self.i += 1
+
+    def peek(self):
+        return self.heap[0][2] if self.heap else None
+
+    def pop(self) -> Request:
+        return self._heapq.heappop(self.heap)[2]
+
+    def next_arrival(self):
+        return self.pending[self.i].arrival if self.i < len(self.pending) else None
+
+    def empty(self) -> bool:
+        return not self.heap and self.i >= len(self.pending)
+
+
+def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
+                residual_interval: int = 50, budget_bytes: int = 0, large_nodes: int = 1 << 19,
+                create_ms: float = 5.0, keep: Optional[set] = None) -> List[Record]:
+    """Run the requests through two batches ("lanes") that advance independently.
+
+    Small requests (fewer than `large_nodes` nodes) go to a lane on a high-priority
+    CUDA stream: its chunks hold only small domains, so they are short, and when
+    SMs free up the scheduler runs its blocks ahead of the other lane's.  Large
+    requests go to a lane on a normal-priority stream.  Each lane runs one chunk
+    at a time; the host polls both without blocking, admits new members at chunk
+    boundaries and, between polls, builds the domains of arrived requests,
+    smallest first, while the device-memory budget allows.  The stop rule, the
+    fields and the step counts are those of `serve_batched` and `Domain.run`.
+    The velocity fields of the requests whose ids are in `keep` are kept in
+    `serve_lanes.fields` (id -> (N, D) array).
+    """
+    import threading
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+    max_it = max_steps - 2
+    records: List[Record] = []
+    lock = threading.Lock()
+    local = threading.local()
+
+    fields = {}
+
+    def collect(r, dom, start, status, t0):
+        if not hasattr(local, "stream"):
+            local.stream = torch.cuda.Stream()
+        _, u, _ = dom.moments(local.stream)
+        rec = Record(r.rid, r.kind, int(np.prod(r.params.n[: r.params.dim])), r.arrival, start, _now(t0),
+                     dom.time_step, status)
+        dom.close()
+        with lock:
+            records.append(rec)
+            if keep and r.rid in keep:
+                fields[r.rid] = u
+
+    arrivals = _Arrivals(reqs)
+    s_init = torch.cuda.Stream()
+    pool = ThreadPoolExecutor(max_workers=4)
+    futures = []
+    host = {"create_s": 0.0, "chunks": [0, 0], "idle_s": 0.0}
+    b0 = Batch(budget_bytes, residual_interval)
+    budget = b0.info()["budget"]
+    b1 = Batch(budget, residual_interval)
+    lanes = [{"batch": b0, "stream": torch.cuda.Stream(priority=-100), "ev": None, "live": {}, "ready": []},
+             {"batch": b1, "stream": torch.cuda.Stream(priority=0), "ev": None, "live": {}, "ready": []}]
+    used = 0
+    t0 = time.perf_counter()
+    try:
+        while not arrivals.empty() or any(ln["live"] or ln["ready"] for ln in lanes):
+            # build the domains of arrived requests (smallest first) while memory allows
+            t1 = time.perf_counter()
+            arrivals.arrive(_now(t0))
+            built = 0
+            while arrivals.peek() is not None and used + arrivals.peek().est_bytes <= budget:
+                r = arrivals.pop()
+                dom = Domain(r.params)
+                dom.init(s_init)
+                lanes[lane_of(r, large_nodes)]["ready"].append((r, dom))
+                used += r.est_bytes
+                built += 1
+                if time.perf_counter() - t1 > create_ms / 1e3:
+                    break
+            if built:
+                s_init.synchronize()
+            host["create_s"] += time.perf_counter() - t1
+            progressed = False
+            for li, ln in enumerate(lanes):
+                if ln["ev"] is not None and not ln["ev"].query():
+                    continue
+                if ln["ev"] is not None:   # its chunk is complete: finished members leave
+                    for dom, status in ln["batch"].poll(wait=False):
+                        r, _, start = ln["live"].pop(dom.h.value)
+                        futures.append(pool.submit(collect, r, dom, start, status, t0))
+                        used -= r.est_bytes
+                    ln["ev"] = None
+                for r, dom in ln["ready"]:
+                    ln["batch"].admit(dom, max_it, tol_density=math.inf, tol_velocity=tol_velocity,
+                                      tol_scalar=math.inf)
+                    ln["live"][dom.h.value] = (r, dom, _now(t0))
+                ln["ready"].clear()
+                if ln["live"]:
+                    ln["batch"].step(1, ln["stream"])
+                    ln["ev"] = torch.cuda.Event()
+                    ln["ev"].record(ln["stream"])
+                    host["chunks"][li] += 1
+                    progressed = True
+            if not progressed:
+                t1 = time.perf_counter()
+                nxt = arrivals.next_arrival()
+                if not any(ln["live"] for ln in lanes) and nxt is not None and arrivals.peek() is None:
+                    time.sleep(max(0.0, min(nxt - _now(t0), 0.01)))
+                else:
+                    time.sleep(0.0002)
+                host["idle_s"] += time.perf_counter() - t1
+        for f in futures:
+            f.result()
+    finally:
+        pool.shutdown(wait=True)
+        b0.close()
+        b1.close()
+    serve_lanes.host_times = host
+    serve_lanes.fields = fields
     return records
 
 

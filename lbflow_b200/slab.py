@@ -186,6 +186,8 @@ class SlabDomain:
         self.stream = stream
         self.dom = Domain(self.params)
         self.dom.set_option(_abi.LBF_OPT_Z_BEGIN, 1).set_option(_abi.LBF_OPT_Z_END, self.nzl + 1)
+        # local plane 1 is global plane z0: nodes round (16-bit storage) as in the whole lattice
+        self.dom.set_option(_abi.LBF_OPT_SEED_OFFSET, (self.z0 - 1) * nx * ny)
         nd, plane, nbytes = C.c_int32(), C.c_int64(), C.c_int64()
         _abi.check(self.dom.lib.lbf_domain_halo_info(self.dom.h, C.byref(nd), C.byref(plane), C.byref(nbytes)))
         self.halo_bytes = nbytes.value

@@ -35,3 +35,19 @@ def test_all_at_once_and_summary():
     assert abs(s["solves_per_s"] - 10.0) < 1e-9
     assert abs(s["p50_s"] - 0.55) < 1e-9 and s["p99_s"] <= 1.0
     assert abs(s["mlups_all_nodes"] - 10 * 100 * 50 / 1e6) < 1e-12
+
+
+def test_lanes_and_smallest_first():
+    reqs = serve.make_requests(200, rate=float("inf"), seed=3)
+    big = [r for r in reqs if serve.request_nodes(r) >= 1 << 19]
+    assert big and all(serve.lane_of(r, 1 << 19) == 1 for r in big)
+    assert all(serve.lane_of(r, 1 << 19) == 0 for r in reqs if r not in big)
+    arr = serve._Arrivals(reqs)
+    arr.arrive(0.0)
+    order = [serve.request_nodes(arr.pop()) for _ in range(len(reqs))]
+    assert order == sorted(order)                      # smallest work first
+    assert arr.empty()
+    timed = serve.make_requests(50, rate=10.0, seed=4)
+    arr = serve._Arrivals(timed)
+    arr.arrive(timed[10].arrival)
+    assert len(arr.heap) == 11 and arr.next_arrival() == timed[11].arrival
