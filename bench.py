@@ -64,8 +64,9 @@ def parse():
     ap.add_argument("--sround", type=int, default=-1, help="16-bit storage: 1/0 stochastic rounding on/off")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the sweep variant and block size by timing candidates first (untimed)")
-    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy", "c4"],
+    ap.add_argument("--workload", default="step", choices=["step", "serve", "batch", "accuracy", "c3", "c4"],
                     help="step: the fused step on one lattice (headline); serve: the serving mix; "
+                         "c3: the D3Q27 central-moment Taylor-Green step (384^3, Re 1600); "
                          "c4: the coupled momentum + scalar step on the packed bed (192x192x384); "
                          "batch: batched vs single-domain sweeps and per-request host costs; "
                          "accuracy: FP32 / FP16 / BF16 storage against FP64 at full size (--case)")
@@ -73,9 +74,16 @@ def parse():
                     help="accuracy: c2 porous channel 256^3 (5000 steps), c3 D3Q27 MRT Taylor-Green 384^3 "
                          "(10000 steps), c4 packed bed with scalar 192x192x384 (20000 steps)")
     ap.add_argument("--acc-steps", type=int, default=0, help="accuracy: override the number of steps")
+    ap.add_argument("--acc-curve", default="",
+                    help="accuracy c2: comma-separated steps; the storages run side by side and the velocity "
+                         "error against FP64 is reported at each (with --acc-n for the lattice side)")
+    ap.add_argument("--acc-n", type=int, default=256, help="accuracy c2 with --acc-curve: lattice side")
     ap.add_argument("--c4-collision", default="trt0.55", choices=["bgk0.6", "bgk0.8", "trt0.8", "trt0.55"],
                     help="accuracy c4: momentum collision (BGK tau 0.6 / 0.8, or TRT tau+ 0.8 / 0.55 magic 1/4)")
     ap.add_argument("--c4-u", type=float, default=0.01, help="accuracy c4: inlet velocity u_z")
+    ap.add_argument("--scalars", type=int, default=1,
+                    help="c4: adsorbing scalars advanced by the one momentum sweep (1..4); with more than one, "
+                         "the same scalars as separate single-scalar domains are timed beside it")
     ap.add_argument("--c3-re", type=float, default=1600.0, help="accuracy c3: Reynolds number of the vortex")
     ap.add_argument("--c3-collision", default="central", choices=["central", "mrt"],
                     help="accuracy c3: central-moment collision (default) or the raw-moment MRT")
@@ -457,6 +465,49 @@ def run_engine(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_c3(args, rank, world, local_rank):
+    """The D3Q27 Taylor-Green vortex step (384^3 periodic, u0 = 0.05, Re = 1600, the
+    central-moment collision, or --c3-collision mrt), FP32 / FP16-deviation / FP64
+    storage: MLUPS and the roofline of the step kernel (read and write 27
+    populations per node, every node fluid, plus 1 B of node type)."""
+    import torch
+    from lbflow_b200 import _abi, cases
+    from lbflow_b200.core import Storage
+    from lbflow_b200.domain import Domain
+    torch.cuda.set_device(local_rank)
+    st = {"f32": Storage.F32, "f64": Storage.F64, "f16dev": Storage.F16DEV, "bf16dev": Storage.BF16DEV}[args.storage]
+    side = 384 if args.n == 256 else args.n
+    p, nu = cases.tgv_d3q27(side, 0.05, args.c3_re, st, collision=args.c3_collision)
+    stream = torch.cuda.current_stream()
+    with Domain(p) as d:
+        configure(d, args, _abi)
+        d.init(stream)
+        sweep = sweep_name(d, _abi)
+        with Clocks(local_rank) as clk:
+            ms = time_steps(d, args.steps, args.warmup, stream, world)
+        clocks = clk.summary()
+        inv = d.inventory()
+    N = side ** 3
+    sec = ms / 1e3
+    alg = N * 2 * 27 * SBYTES[args.storage] + N
+    peak, kind = peaks()
+    achieved = alg / (sec / args.steps) / 1e9
+    if rank != 0:
+        return
+    line = {"metric": "MLUPS", "value": world * N * args.steps / sec / 1e6, "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if st == Storage.F64 else "f32",
+            "data": "synthetic (analytic initial field)",
+            "config": {"workload": f"D3Q27 Taylor-Green vortex {side}^3 periodic, u0 0.05, Re {args.c3_re:g}, "
+                                   f"{args.c3_collision} collision (tau {3 * nu + 0.5:.5f})",
+                       "storage": args.storage, "sweep": sweep,
+                       "l2": f"inputs larger than L2 (populations 2 x 27 x {SBYTES[args.storage]} B per node)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "peak_source": kind, "algorithmic_bytes_per_launch": alg},
+            "finite_after_run": bool(np.all(np.isfinite(inv))), "gpu_launches": args.steps, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def run_c4(args, rank, world, local_rank):
     """The coupled D3Q19 momentum + passive-scalar step with Langmuir adsorption on
     the packed bed (192 x 192 x 384, porosity 0.6 of seeded overlapping spheres
@@ -467,7 +518,9 @@ def run_c4(args, rank, world, local_rank):
     FP32 or FP64 storage: MFLUPS and the roofline of the step kernels.
     Algorithmic bytes per fluid update: 2 Q s for f and 2 Q s for g, plus q_ads and
     the previous scalar value read and written at each bounce-back node (4 s),
-    plus 1 B of node type per node."""
+    plus 1 B of node type per node.  With --scalars K, K scalars (adsorption rates
+    k_a 1e-3 (1 + i)) share the momentum sweep: 2 Q s (1 + K) per fluid update and
+    4 s K per bounce-back node."""
     import torch
     from lbflow_b200 import _abi, cases
     from lbflow_b200.core import Storage
@@ -492,9 +545,23 @@ def run_c4(args, rank, world, local_rank):
     from lbflow_b200.core import BGK, TRT
     coll = {"bgk0.6": BGK(0.6), "bgk0.8": BGK(0.8), "trt0.8": TRT.from_magic(0.8, 0.25),
             "trt0.55": TRT.from_magic(0.55, 0.25)}[args.c4_collision]
-    mp, sp = cases.packed_bed_scalar(n, mask=mask, storage=st, u_in=args.c4_u, tau_g=0.55, collision=coll)
+    K = max(1, min(4, args.scalars))
+    sps = []
+    for i in range(K):
+        mp, sp = cases.packed_bed_scalar(n, mask=mask, storage=st, u_in=args.c4_u, tau_g=0.55, collision=coll,
+                                         ka=1e-3 * (1 + i))
+        sps.append(sp)
     stream = torch.cuda.current_stream()
-    with Domain(mp, sp) as d:
+    separate_ms = None
+    if K > 1:
+        # the reference's cost model on this engine: one full domain per scalar
+        separate_ms = 0.0
+        for sp in sps:
+            with Domain(mp, sp) as d1:
+                configure(d1, args, _abi)
+                d1.init(stream)
+                separate_ms += time_steps(d1, args.steps, args.warmup, stream, world)
+    with Domain(mp, sps) as d:
         configure(d, args, _abi)
         d.init(stream)
         cls, _ = d.node_class()
@@ -509,7 +576,7 @@ def run_c4(args, rank, world, local_rank):
         finite = bool(np.all(np.isfinite(inv)))
     sec = ms / 1e3
     s_b = 8 if st == Storage.F64 else 4
-    alg = n_fluid * 4 * 19 * s_b + n_bb * 4 * s_b + mask.size
+    alg = n_fluid * 2 * 19 * s_b * (1 + K) + n_bb * 4 * s_b * K + mask.size
     peak, kind = peaks()
     achieved = alg / (sec / args.steps) / 1e9
     if rank != 0:
@@ -518,15 +585,21 @@ def run_c4(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if st == Storage.F64 else "f32",
             "data": "synthetic (seeded sphere packing)",
-            "config": {"workload": "coupled D3Q19 momentum + D3Q19 scalar with Langmuir adsorption, packed bed "
-                                   f"{side}x{side}x{2 * side}, porosity 0.6 (8 clear layers at each end), Zou-He inlet "
-                                   f"u_z={args.c4_u:g}, momentum {args.c4_collision}, scalar tau 0.55",
+            "config": {"workload": f"coupled D3Q19 momentum + {K} D3Q19 scalar{'s' if K > 1 else ''} with Langmuir "
+                                   f"adsorption, packed bed {side}x{side}x{2 * side}, porosity 0.6 (8 clear layers at "
+                                   f"each end), Zou-He inlet u_z={args.c4_u:g}, momentum {args.c4_collision}, "
+                                   "scalar tau 0.55",
+                       "scalars": K,
                        "storage": "f64" if st == Storage.F64 else "f32", "n_fluid": n_fluid,
                        "bounce_back_nodes": n_bb, "sweep": sweep,
                        "l2": "inputs larger than L2 (f and g populations, 2 buffers each)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "peak_source": kind, "algorithmic_bytes_per_launch": alg},
             "finite_after_run": finite, "gpu_launches": args.steps * 2, "clocks": clocks}
+    if separate_ms is not None:
+        line["separate_domains"] = {"ms_per_step": separate_ms / args.steps,
+                                    "note": f"the {K} scalars as {K} single-scalar domains, each with its own "
+                                            "momentum sweep, timed one after another"}
     print(json.dumps(line), flush=True)
 
 
@@ -704,6 +777,37 @@ def run_accuracy(args, rank, world, local_rank):
         return float(np.linalg.norm(a - b)) / (nb if nb > 0 else 1.0)
 
     out = {"workload": f"accuracy {args.case}", "n_gpus": 1, "runs": {}}
+    if args.case == "c2" and args.acc_curve:
+        # the storages side by side: velocity error against FP64 at each listed step
+        n = args.acc_n
+        mask = geometry(n, args.seed, 0.7)
+        fl = mask == 0
+        marks = sorted(int(x) for x in args.acc_curve.split(","))
+        stores = [Storage.F64, Storage.F32, Storage.F16DEV, Storage.BF16DEV]
+        doms = {}
+        for st in stores:
+            d = Domain(cases.porous_channel_d3q19([n] * 3, mask=mask, force=1e-6, storage=st))
+            if args.sround >= 0:
+                d.set_option(_abi.LBF_OPT_SROUND, args.sround)
+            doms[st] = d.init()
+        out["case"] = (f"C2 geometry on {n}^3 (D3Q19 TRT tau+ 0.8 magic 1/4, g_x 1e-6, spheres r in [4,10], "
+                       f"porosity 0.7, seed {args.seed})")
+        out["sround"] = None if args.sround < 0 else args.sround
+        out["curve"] = []
+        t = 0
+        for mark in marks:
+            for d in doms.values():
+                d.step(mark - t)
+            t = mark
+            ref = doms[Storage.F64].moments()[1][fl]
+            row = {"step": mark}
+            for st in stores[1:]:
+                row[st.name] = rel(doms[st].moments()[1][fl], ref)
+            out["curve"].append(row)
+        for d in doms.values():
+            d.close()
+        print(json.dumps(out), flush=True)
+        return
     if args.case == "c2":
         steps = args.acc_steps or 5000
         mask = geometry(256, args.seed, 0.7)
@@ -890,6 +994,8 @@ def main():
         run_serve(args, rank, world, local_rank)
     elif args.workload == "batch":
         run_batch_probe(args, rank, world, local_rank)
+    elif args.workload == "c3":
+        run_c3(args, rank, world, local_rank)
     elif args.workload == "c4":
         run_c4(args, rank, world, local_rank)
     elif args.workload == "accuracy":

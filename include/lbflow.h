@@ -33,6 +33,7 @@ extern "C" {
 #endif
 
 #define LBF_ABI_VERSION 1
+#define LBF_MAX_SCALARS 4   /* passive scalars one domain advances in its momentum sweep */
 
 typedef enum {
     LBF_OK = 0,
@@ -181,7 +182,12 @@ lbf_status lbf_velocity_set_tables(int32_t velocity_set, int32_t* d, int32_t* q,
 /* ---- one domain (replaces momentum::Lattice + passive_scalar::Lattice) ---- */
 /* Lattice::new (src/momentum/lattice.rs:27-207). */
 lbf_status lbf_domain_create(const lbf_domain_desc* desc, lbf_domain** out);
-/* passive_scalar::Lattice::new (src/passive_scalar/lattice.rs:26-181). One scalar per domain. */
+/* passive_scalar::Lattice::new (src/passive_scalar/lattice.rs:26-181).  Up to
+ * LBF_MAX_SCALARS calls per domain, before lbf_domain_init: the scalars of
+ * passive_scalar::LatticeVec (src/passive_scalar/lattice.rs:353-430), numbered in
+ * attach order.  One momentum sweep advances all of them: each step updates the
+ * momentum populations of a node, then each scalar's in turn.  Scalars interact
+ * only through the shared velocity, as in the reference. */
 lbf_status lbf_scalar_attach(lbf_domain* dom, const lbf_scalar_desc* desc);
 /* Lattice::initialize_nodes (src/momentum/lattice.rs:322-328,
  * src/passive_scalar/lattice.rs:241-246): f = f_eq(rho0, u0) on fluid nodes. */
@@ -198,17 +204,24 @@ lbf_status lbf_domain_step(lbf_domain* dom, int64_t nsteps, int64_t residual_int
 lbf_status lbf_domain_run(lbf_domain* dom, int64_t max_iterations, int64_t residual_interval,
                           double tolerance_density, double tolerance_velocity,
                           double tolerance_scalar, int64_t* steps_done, void* stream);
-/* Residuals of the last residual step: [density, velocity_x.., scalar] (1+D+S entries).
- * Synchronous.  *time_step receives the step they belong to (-1 if none yet). */
+/* Residuals of the last residual step: [density, velocity_x.., scalar_0, scalar_1 ..]
+ * (1 + D + number of scalars entries).  Synchronous.  *time_step receives the step
+ * they belong to (-1 if none yet). */
 lbf_status lbf_domain_residuals(lbf_domain* dom, double* out, int64_t* time_step);
 /* Moments at the current time step (what write_data stores in data/<t>/,
- * src/momentum/io.rs:74-192): density[N], velocity[N*D], scalar[N] (host
- * pointers, any may be NULL).  Solid nodes report their initial values. */
+ * src/momentum/io.rs:74-192): density[N], velocity[N*D], scalar[N] of scalar 0
+ * (host pointers, any may be NULL).  Solid nodes report their initial values. */
 lbf_status lbf_domain_get_moments(lbf_domain* dom, double* density, double* velocity,
                                   double* scalar, void* stream);
-/* Adsorbed amount q_ads per node (0 where not a bounce-back node). Host pointer. */
+/* Scalar `index` (attach order) at the current time step, scalar[N] (host pointer;
+ * passive_scalar/io.rs write_data of that lattice). */
+lbf_status lbf_domain_get_scalar(lbf_domain* dom, int32_t index, double* scalar, void* stream);
+/* Adsorbed amount q_ads per node of scalar 0 (0 where not a bounce-back node). Host pointer. */
 lbf_status lbf_domain_get_q_ads(lbf_domain* dom, double* q_ads);
-/* FP64 inventories over fluid nodes: [sum rho, sum rho*u (D), sum C, sum q_ads]. */
+/* The same for scalar `index`. */
+lbf_status lbf_domain_get_q_ads_at(lbf_domain* dom, int32_t index, double* q_ads);
+/* FP64 inventories over fluid nodes: [sum rho, sum rho*u (D), sum C, sum q_ads] (C, q_ads
+ * of scalar 0). */
 lbf_status lbf_domain_inventory(lbf_domain* dom, double* out, void* stream);
 /* Node classes (LBF_CLASS_* bits) and solid-neighbour link masks (bit i: the
  * neighbour along c_i is solid), computed on the device. */

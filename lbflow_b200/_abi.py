@@ -27,6 +27,7 @@ LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
 (LBF_OPT_BLOCK_X, LBF_OPT_STAGE, LBF_OPT_PIPE, LBF_OPT_PIPE_STAGES, LBF_OPT_COMPACT, LBF_OPT_Z_BEGIN, LBF_OPT_Z_END,
  LBF_OPT_SPARSE, LBF_OPT_STREAMING, LBF_OPT_SROUND, LBF_OPT_WAIT_LIMIT, LBF_OPT_SEED_OFFSET) = range(12)
 LBF_STREAM_PULL, LBF_STREAM_PUSH, LBF_STREAM_INPLACE = range(3)
+LBF_MAX_SCALARS = 4
 
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2
@@ -99,6 +100,8 @@ SIGNATURES = {
     "lbf_domain_residuals": (_I32, [_P, _PD, _PI64]),
     "lbf_domain_get_moments": (_I32, [_P, _PD, _PD, _PD, _P]),
     "lbf_domain_get_q_ads": (_I32, [_P, _PD]),
+    "lbf_domain_get_scalar": (_I32, [_P, _I32, _PD, _P]),
+    "lbf_domain_get_q_ads_at": (_I32, [_P, _I32, _PD]),
     "lbf_domain_inventory": (_I32, [_P, _PD, _P]),
     "lbf_domain_get_node_class": (_I32, [_P, _PU32, _PU32]),
     "lbf_domain_time_step": (_I32, [_P, _PI64]),

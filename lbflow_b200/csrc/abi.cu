@@ -5,6 +5,7 @@
 // by anti-bounce-back and extrapolated wall velocities, the per-node moments of
 // residual steps, and the FP64 partial-sum slots of the reductions.
 #include <cuda_runtime.h>
+#include <sys/mman.h>
 
 #include <algorithm>
 #include <cmath>
@@ -50,7 +51,8 @@ size_t rt_bytes(int st) { return st == LBF_STORE_F64 ? 8 : 4; }   // compute typ
 // the widest launch a domain can make (the dense sweep at 32 threads per block,
 // plus one face pass per face at 32 threads per block: an upper bound of every
 // other launch shape, 256-thread sparse and inventory sweeps included).
-constexpr int ACCUM_PLANES = 6;
+constexpr int ACCUM_PLANES = 4 + NSMAX;   // residual accumulators of a scalar sweep (the most)
+static_assert(NSMAX == LBF_MAX_SCALARS, "the header's scalar limit is the kernels'");
 long long accum_slots(const long long* n, int nfaces) {
     long long s = (n[0] + 31) / 32 * n[1] * n[2];
     const long long N = n[0] * n[1] * n[2];
@@ -155,7 +157,7 @@ cudaEvent_t g_stage_ev[2] = {nullptr, nullptr};
 
 void host_copy_parallel(char* dst, const char* src, size_t bytes) {
     const size_t per = 4u << 20;
-    const int nt = (int)std::min<size_t>(std::max(1u, std::min(16u, std::thread::hardware_concurrency())),
+    const int nt = (int)std::min<size_t>(std::max(1u, std::min(32u, std::thread::hardware_concurrency())),
                                          (bytes + per - 1) / per);
     if (nt <= 1) {
         std::memcpy(dst, src, bytes);
@@ -174,6 +176,13 @@ cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (bytes < (4u << 20)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
         return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    }
+    // fresh caller memory is faulted in by the copy: ask for huge pages (a hint,
+    // ignored where transparent huge pages are off) to cut the page faults
+    {
+        const uintptr_t a = ((uintptr_t)dst + (2u << 20) - 1) & ~(uintptr_t)((2u << 20) - 1);
+        const uintptr_t b = ((uintptr_t)dst + bytes) & ~(uintptr_t)((2u << 20) - 1);
+        if (b > a) madvise((void*)a, b - a, MADV_HUGEPAGE);
     }
     std::lock_guard<std::mutex> lk(g_stage_mu);
     if (!g_stage[0]) {
@@ -288,26 +297,30 @@ struct lbf_domain {
     long long N = 0;
     unsigned long long n_fluid = 0, n_bb = 0;
     bool facebc = false, prepared = false, initialized = false;
+    unsigned folded = 0;   // no-slip faces applied through the link bits of the pull
     // host copies of the inputs (solid-node outputs, re-initialisation)
     std::vector<uint8_t> type;
-    std::vector<double> rho0, u0, c0;
-    double rho0u = 1.0, u0u[3] = {0, 0, 0}, c0u = 0.0;
-    // scalar
-    bool scalar = false;
-    lbf_scalar_desc sdesc{};
+    std::vector<double> rho0, u0;
+    double rho0u = 1.0, u0u[3] = {0, 0, 0};
+    // passive scalars (passive_scalar::LatticeVec): one momentum sweep advances all
+    int ns = 0;
+    bool scalar = false;          // ns > 0
+    lbf_scalar_desc sdesc[NSMAX] = {};
+    std::vector<double> c0[NSMAX];   // per-node initial scalar (host copy), or empty
     // device memory
     void* pop[2] = {nullptr, nullptr};
-    void* gpop[2] = {nullptr, nullptr};
+    void* gpop[NSMAX][2] = {};
     uint32_t* mask = nullptr;
     uint8_t* dtype = nullptr;
     void* mom[2] = {nullptr, nullptr};
     void* pb[6][2] = {};
-    void* snap[6] = {};
-    unsigned outflow = 0;   // faces with a scalar extrapolation outflow (face pass)
+    void* snap[NSMAX][6] = {};
+    unsigned outflow = 0;   // faces with a scalar extrapolation outflow of any scalar (face pass)
+    unsigned outflow_s[NSMAX] = {};
     long long pb_plane[6] = {0, 0, 0, 0, 0, 0};
-    void* qads = nullptr;
-    void* cprev = nullptr;
-    double* c_init_dev = nullptr;
+    void* qads[NSMAX] = {};
+    void* cprev[NSMAX] = {};
+    double* c_init_dev[NSMAX] = {};
     double* accum = nullptr;      // per-block partial sums: [accumulator][accum_cap]
     long long accum_cap = 0;      // slots per accumulator (the most blocks any launch of the domain uses)
     long long slot_next = 0;      // next free slot of the step being launched
@@ -350,16 +363,25 @@ struct lbf_domain {
 
     ~lbf_domain() {
         for (int k = 0; k < 2; ++k) {
-            dev_free(pop[k], dev); dev_free(gpop[k], dev); dev_free(mom[k], dev);
+            dev_free(pop[k], dev); dev_free(mom[k], dev);
             for (int f = 0; f < 6; ++f) dev_free(pb[f][k], dev);
         }
-        for (int f = 0; f < 6; ++f) dev_free(snap[f], dev);
-        for (void* p : {(void*)mask, (void*)dtype, qads, cprev, (void*)c_init_dev, (void*)accum, (void*)res_dev,
+        for (int si = 0; si < NSMAX; ++si) {
+            dev_free(gpop[si][0], dev); dev_free(gpop[si][1], dev);
+            for (int f = 0; f < 6; ++f) dev_free(snap[si][f], dev);
+            dev_free(qads[si], dev); dev_free(cprev[si], dev); dev_free(c_init_dev[si], dev);
+        }
+        for (void* p : {(void*)mask, (void*)dtype, (void*)accum, (void*)res_dev,
                         (void*)obs, (void*)counts, (void*)err, (void*)list, (void*)fmask, (void*)rw})
             dev_free(p, dev);
         pinned64_free(res_host);
     }
-    int nfields() const { return 1 + d + (scalar ? 1 : 0); }
+    // per-node moment fields: rho, u_0..u_{d-1}, one per scalar
+    int nfields() const { return 1 + d + ns; }
+    // residual accumulators of the step kernel: rho, u_0..u_2, then one per scalar slot
+    int nacc() const { return ns > 0 ? 4 + NSMAX : 5; }
+    // fields of a face layer: u_0..u_{d-1}, then one per scalar (at least one)
+    int pb_nf() const { return d + std::max(ns, 1); }
 };
 
 namespace {
@@ -417,7 +439,8 @@ bool mom_kind_ok(const lbf_domain_desc& ds, int vs, int f, std::string& why) {
 void fill_face_params(const lbf_domain* D, StepParams& P) {
     for (int f = 0; f < 6; ++f) {
         const lbf_bc_desc& b = D->desc.bc[f];
-        P.face[f].kind = f < D->nfaces ? b.kind : BC_PERIODIC;
+        // a folded face has no explicit rule left: the pull's link bits apply it
+        P.face[f].kind = f < D->nfaces && !(D->folded >> f & 1u) ? b.kind : BC_PERIODIC;
         P.face[f].has_rho = b.has_density;
         for (int a = 0; a < 3; ++a) { P.face[f].has_u[a] = b.has_velocity[a]; P.face[f].u[a] = b.velocity[a]; }
         P.face[f].rho = b.density;
@@ -426,11 +449,11 @@ void fill_face_params(const lbf_domain* D, StepParams& P) {
     bool zero = true;
     for (int f = 0; f < 6; ++f) zero = zero && D->desc.face_order[f] == 0;
     for (int o = 0; o < 6; ++o) P.order[o] = zero ? o : D->desc.face_order[o];
-    if (D->scalar) {
+    for (int si = 0; si < D->ns; ++si) {
         for (int f = 0; f < 6; ++f) {
-            const lbf_scalar_bc_desc& s = D->sdesc.bc[f];
-            SFaceBC& o = P.sface[f];
-            o.kind = f < D->nfaces ? s.kind : SBC_PERIODIC;
+            const lbf_scalar_bc_desc& s = D->sdesc[si].bc[f];
+            SFaceBC& o = P.sc[si].face[f];
+            o.kind = f < D->nfaces && !(D->folded >> f & 1u) ? s.kind : SBC_PERIODIC;
             o.unknown_only = s.unknown_populations_only;
             o.value = s.scalar_value;
             // wall velocity from the momentum BC of the same face (ps/bc.rs:43-59)
@@ -448,21 +471,32 @@ void fill_face_params(const lbf_domain* D, StepParams& P) {
     }
 }
 
+// Scalars with adsorption, one bit each (checkpoint header).
+int32_t ads_bits(const lbf_domain* D) {
+    int32_t b = 0;
+    for (int si = 0; si < D->ns; ++si) if (D->qads[si]) b |= 1 << si;
+    return b;
+}
+
+// Observed moments (doubles, N each): rho, u_0..u_{d-1}, one per scalar (at least one).
+int obs_fields(const lbf_domain* D) { return 1 + D->d + std::max(D->ns, 1); }
+
 bool face_needs_layers(const lbf_domain* D, int f) {
     if (f >= D->nfaces) return false;
     if (D->desc.bc[f].kind == LBF_BC_ANTI_BOUNCE_BACK) return true;
-    if (!D->scalar) return false;
-    const int k = D->sdesc.bc[f].kind;
-    if (k == LBF_SBC_ANTI_BB_NO_FLUX) return true;
-    if (k == LBF_SBC_ANTI_BOUNCE_BACK) {
-        const lbf_bc_desc& m = D->desc.bc[f];
-        if (m.kind == LBF_BC_NO_SLIP || m.kind == LBF_BC_BOUNCE_BACK) return false;
-        if (m.kind == LBF_BC_ZOU_HE) {
-            bool all = true;
-            for (int a = 0; a < D->d; ++a) all = all && m.has_velocity[a];
-            return !all;
+    for (int si = 0; si < D->ns; ++si) {
+        const int k = D->sdesc[si].bc[f].kind;
+        if (k == LBF_SBC_ANTI_BB_NO_FLUX) return true;
+        if (k == LBF_SBC_ANTI_BOUNCE_BACK) {
+            const lbf_bc_desc& m = D->desc.bc[f];
+            if (m.kind == LBF_BC_NO_SLIP || m.kind == LBF_BC_BOUNCE_BACK) continue;
+            if (m.kind == LBF_BC_ZOU_HE) {
+                bool all = true;
+                for (int a = 0; a < D->d; ++a) all = all && m.has_velocity[a];
+                if (all) continue;
+            }
+            return true;
         }
-        return true;
     }
     return false;
 }
@@ -573,31 +607,32 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     const bool inplace = whole && scheme == LBF_STREAM_INPLACE;
     D->push = whole && scheme == LBF_STREAM_PUSH;
     void* np[2] = {nullptr, nullptr};
-    void* ng[2] = {nullptr, nullptr};
+    void* ng[NSMAX][2] = {};
     const size_t rb = rt_bytes(D->st);
     if (e == cudaSuccess) e = dev_alloc(&np[0], (size_t)D->q * Fp * eb, D->dev);
     if (e == cudaSuccess && !inplace) e = dev_alloc(&np[1], (size_t)D->q * Fp * eb, D->dev);
-    for (int k = 0; k < 2 && e == cudaSuccess && D->scalar; ++k) e = dev_alloc(&ng[k], (size_t)D->q * Fp * rb, D->dev);
+    for (int si = 0; si < D->ns; ++si)
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = dev_alloc(&ng[si][k], (size_t)D->q * Fp * rb, D->dev);
     if (e != cudaSuccess) {
         dev_free(flist, D->dev); dev_free(np[0], D->dev); dev_free(np[1], D->dev);
-        dev_free(ng[0], D->dev); dev_free(ng[1], D->dev);
+        for (int si = 0; si < D->ns; ++si) { dev_free(ng[si][0], D->dev); dev_free(ng[si][1], D->dev); }
         dev_free(D->fmask, D->dev); dev_free(D->rw, D->dev);
         D->fmask = nullptr; D->rw = nullptr;
         cudaGetLastError();
         return fail(e == cudaErrorMemoryAllocation ? LBF_ENOMEM : LBF_EDEVICE,
                     std::string("sparse layout: ") + cudaGetErrorString(e));
     }
-    const long long old_bytes = 2ll * D->q * D->Np * (long long)eb;
+    const long long old_bytes = D->pop[0] ? 2ll * D->q * D->Np * (long long)eb : 0;
     dev_free(D->pop[0], D->dev);
     dev_free(D->pop[1], D->dev);
     D->pop[0] = np[0];
     D->pop[1] = np[1];
-    if (D->scalar) {
-        const long long old_g = 2ll * D->q * D->Np * (long long)rb;
-        dev_free(D->gpop[0], D->dev);
-        dev_free(D->gpop[1], D->dev);
-        D->gpop[0] = ng[0];
-        D->gpop[1] = ng[1];
+    for (int si = 0; si < D->ns; ++si) {
+        const long long old_g = D->gpop[si][0] ? 2ll * D->q * D->Np * (long long)rb : 0;
+        dev_free(D->gpop[si][0], D->dev);
+        dev_free(D->gpop[si][1], D->dev);
+        D->gpop[si][0] = ng[si][0];
+        D->gpop[si][1] = ng[si][1];
         D->bytes += 2ll * D->q * Fp * (long long)rb - old_g;
     }
     D->Np = Fp;
@@ -608,6 +643,46 @@ lbf_status build_sparse(lbf_domain* D, cudaStream_t s) {
     D->rw_w = W;
     D->sparse = true;
     return st;
+}
+
+// A no-slip face (bc.rs NoSlip: f[ibar] = f*[i] of the node itself for each i
+// leaving through the face) is the inner bounce-back of a solid layer beyond the
+// face, so the pull applies it through the node's link bits.  Among explicit
+// faces that is exact when the folded rule would run first at every node it
+// shares with an explicit face, i.e. the face precedes, in the face order, each
+// explicit face that meets it along an edge (folded rules read only the node's
+// own post-collision slots, so they commute with one another).  With a scalar
+// the scalar rule of the face must be the same bounce-back (BBNoFlux) and the
+// inner rule InnerBounceBack, which the link bits apply to the scalar.
+// Folding keeps the long face code off the bulk of the lattice: only nodes on
+// the remaining explicit faces run it.
+unsigned foldable_faces(const lbf_domain* D, unsigned expl) {
+    int pos[6] = {0, 1, 2, 3, 4, 5};
+    bool zero = true;
+    for (int f = 0; f < 6; ++f) zero = zero && D->desc.face_order[f] == 0;
+    if (!zero)
+        for (int o = 0; o < D->nfaces; ++o)
+            if (D->desc.face_order[o] >= 0 && D->desc.face_order[o] < 6) pos[D->desc.face_order[o]] = o;
+    unsigned cand = 0;
+    for (int f = 0; f < D->nfaces; ++f) {
+        if (D->desc.bc[f].kind != LBF_BC_NO_SLIP) continue;
+        bool same = true;
+        for (int si = 0; si < D->ns; ++si)
+            same = same && D->sdesc[si].bc[f].kind == LBF_SBC_BB_NO_FLUX &&
+                   D->sdesc[si].inner_boundary_condition == LBF_INNER_BOUNCE_BACK;
+        if (same) cand |= 1u << f;
+    }
+    unsigned fold = 0;
+    for (int f = 0; f < D->nfaces; ++f) {
+        if (!(cand >> f & 1u)) continue;
+        bool ok = true;
+        for (int g = 0; g < D->nfaces; ++g) {
+            const bool meets = g / 2 != f / 2 || (g != f && D->n[f / 2] == 1);
+            if ((expl >> g & 1u) && !(cand >> g & 1u) && meets && pos[g] < pos[f]) ok = false;
+        }
+        if (ok) fold |= 1u << f;
+    }
+    return fold;
 }
 
 // Node classification + device masks (Lattice::new), run once before init.
@@ -622,11 +697,18 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
     for (int f = 0; f < D->nfaces; ++f) {
         const int k = D->desc.bc[f].kind;
         if (D->facebc) {
-            if (k != LBF_BC_PERIODIC || (D->scalar && D->sdesc.bc[f].kind != LBF_SBC_PERIODIC)) expl |= 1u << f;
+            bool sper = true;
+            for (int si = 0; si < D->ns; ++si) sper = sper && D->sdesc[si].bc[f].kind == LBF_SBC_PERIODIC;
+            if (k != LBF_BC_PERIODIC || !sper) expl |= 1u << f;
         } else if (k == LBF_BC_NO_SLIP) {
             fold |= 1u << f;
         }
     }
+    if (D->facebc) {
+        fold = foldable_faces(D, expl);
+        expl &= ~fold;
+    }
+    D->folded = fold;
     uint32_t* cls = nullptr;
     uint32_t* links = nullptr;
     lbf_status st;
@@ -663,11 +745,13 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
         const long long plane = D->pb_plane[f];
         if (face_needs_layers(D, f))
             for (int k = 0; k < 2; ++k)
-                if (!D->pb[f][k] && (st = dmalloc(D, &D->pb[f][k], 2 * (D->d + 1) * plane * rt_bytes(D->st)))) return st;
-        if ((D->outflow >> f & 1u) && !D->snap[f]) {
-            const size_t b = 2 * (size_t)D->q * plane * rt_bytes(D->st);
-            if ((st = dmalloc(D, &D->snap[f], b))) return st;
-            CK(cudaMemsetAsync(D->snap[f], 0, b, s));   // solid neighbours read as zero populations
+                if (!D->pb[f][k] && (st = dmalloc(D, &D->pb[f][k], 2 * D->pb_nf() * plane * rt_bytes(D->st)))) return st;
+        for (int si = 0; si < D->ns; ++si) {
+            if ((D->outflow_s[si] >> f & 1u) && !D->snap[si][f]) {
+                const size_t b = 2 * (size_t)D->q * plane * rt_bytes(D->st);
+                if ((st = dmalloc(D, &D->snap[si][f], b))) return st;
+                CK(cudaMemsetAsync(D->snap[si][f], 0, b, s));   // solid neighbours read as zero populations
+            }
         }
     }
     if (D->sparse) {             // already laid out (a repeated classification keeps the state)
@@ -687,6 +771,13 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
             D->prepared = true;
             return LBF_OK;
         }
+    }
+    // the dense layout: A/B population buffers of every node (and the scalar's)
+    for (int k = 0; k < 2; ++k) {
+        if (!D->pop[k] && (st = dmalloc(D, &D->pop[k], (size_t)D->q * D->Np * st_bytes(D->st)))) return st;
+        for (int si = 0; si < D->ns; ++si)
+            if (!D->gpop[si][k] && (st = dmalloc(D, &D->gpop[si][k], (size_t)D->q * D->Np * rt_bytes(D->st))))
+                return st;
     }
     const bool want = (D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0) && !z_restricted(D);
     D->compact = want;
@@ -746,30 +837,30 @@ void base_params(const lbf_domain* D, StepParams& P, long long t) {
         P.pb_dst[f] = D->pb[f][t & 1];
         if (D->pb[f][0]) P.any_face = 1;
     }
-    for (int f = 0; f < 6; ++f) P.snap[f] = D->snap[f];
     P.mom_prev = D->mom[(t + 1) & 1];
     P.mom_cur = D->mom[t & 1];
     P.accum = D->accum;
     P.accum_stride = D->accum_cap;
     P.slot0 = 0;
-    if (D->scalar) {
-        const lbf_scalar_desc& s = D->sdesc;
-        P.has_scalar = 1;
-        P.s_coll = s.collision.kind; P.s_inner = s.inner_boundary_condition; P.s_has_source = s.has_source;
-        P.s_tau = s.collision.tau; P.s_omega = s.collision.kind == LBF_BGK ? 1.0 / s.collision.tau : 0.0;
-        P.s_bgk_cb = s.collision.kind == LBF_BGK ? 1.0 - 0.5 / s.collision.tau : 0.0;
-        P.s_op = s.collision.omega_plus; P.s_om = s.collision.omega_minus; P.s_source = s.source_value;
-        P.s_ads = s.has_adsorption;
-        P.ka = s.adsorption_rate; P.kd = s.desorption_rate; P.qmax = s.q_max;
-        P.c_solid = s.initial_scalar_value;
-        P.c_init = D->c_init_dev;
-        const size_t rb = rt_bytes(D->st);
-        for (int i = 0; i < D->q; ++i) {
-            P.gsrcp[i] = (const char*)D->gpop[t & 1] + (size_t)i * D->Np * rb;
-            P.gdstp[i] = (char*)D->gpop[(t + 1) & 1] + (size_t)i * D->Np * rb;
-        }
-        P.qads = D->qads;
-        P.cprev = D->cprev;
+    P.pb_nf = D->pb_nf();
+    P.has_scalar = D->ns > 0 ? 1 : 0;
+    P.nscalar = D->ns;
+    for (int si = 0; si < D->ns; ++si) {
+        const lbf_scalar_desc& s = D->sdesc[si];
+        ScalarParams& o = P.sc[si];
+        o.coll = s.collision.kind; o.inner = s.inner_boundary_condition; o.has_source = s.has_source;
+        o.tau = s.collision.tau; o.omega = s.collision.kind == LBF_BGK ? 1.0 / s.collision.tau : 0.0;
+        o.bgk_cb = s.collision.kind == LBF_BGK ? 1.0 - 0.5 / s.collision.tau : 0.0;
+        o.op = s.collision.omega_plus; o.om = s.collision.omega_minus; o.source = s.source_value;
+        o.ads = s.has_adsorption;
+        o.ka = s.adsorption_rate; o.kd = s.desorption_rate; o.qmax = s.q_max;
+        o.c_solid = s.initial_scalar_value;
+        o.c_init = D->c_init_dev[si];
+        o.gsrc = D->gpop[si][t & 1];
+        o.gdst = D->gpop[si][(t + 1) & 1];
+        o.qads = D->qads[si];
+        o.cprev = D->cprev[si];
+        for (int f = 0; f < 6; ++f) o.snap[f] = D->snap[si][f];
     }
 }
 
@@ -965,20 +1056,20 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     InitParams I{};
     I.rho0 = D->rho0u;
     for (int a = 0; a < 3; ++a) I.u0[a] = D->u0u[a];
-    I.c0 = D->scalar ? D->sdesc.initial_scalar_value : 0.0;
-    I.q0 = D->scalar ? D->sdesc.initial_q_ads : 0.0;
+    for (int si = 0; si < D->ns; ++si) {
+        I.c0[si] = D->sdesc[si].initial_scalar_value;
+        I.q0[si] = D->sdesc[si].initial_q_ads;
+        I.c_field[si] = D->c_init_dev[si];   // the per-node initial scalar, resident since attach
+    }
     // upload per-node initial fields for the duration of the init kernel
     double* tmp = nullptr;
     const size_t nr = D->rho0.empty() ? 0 : D->N, nu = D->u0.empty() ? 0 : D->N * D->d;
-    const size_t nc = D->c0.empty() ? 0 : D->N;
-    if (nr + nu + nc) {
-        CK(dev_alloc((void**)&tmp, (nr + nu + nc) * sizeof(double), D->dev));
+    if (nr + nu) {
+        CK(dev_alloc((void**)&tmp, (nr + nu) * sizeof(double), D->dev));
         if (nr) CK(cudaMemcpyAsync(tmp, D->rho0.data(), nr * 8, cudaMemcpyHostToDevice, s));
         if (nu) CK(cudaMemcpyAsync(tmp + nr, D->u0.data(), nu * 8, cudaMemcpyHostToDevice, s));
-        if (nc) CK(cudaMemcpyAsync(tmp + nr + nu, D->c0.data(), nc * 8, cudaMemcpyHostToDevice, s));
         I.rho_field = nr ? tmp : nullptr;
         I.u_field = nu ? tmp + nr : nullptr;
-        I.c_field = nc ? tmp + nr + nu : nullptr;
     }
     void* pb[12];
     for (int f = 0; f < 6; ++f) { pb[2 * f] = D->pb[f][0]; pb[2 * f + 1] = D->pb[f][1]; }
@@ -1029,7 +1120,7 @@ lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s
         cudaError_t e = launch_step_any(D, P, s);
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
         if (P.residual) {
-            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, 5, 1, D->res_dev);
+            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, D->nacc(), 1, D->res_dev);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(D->res_host, D->res_dev, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
             D->res_step = t;
@@ -1044,7 +1135,7 @@ lbf_status do_observe(lbf_domain* D, cudaStream_t s) {
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called first");
     if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     lbf_status st;
-    if (!D->obs && (st = dmalloc(D, (void**)&D->obs, (size_t)D->N * (D->d + 2) * sizeof(double)))) return st;
+    if (!D->obs && (st = dmalloc(D, (void**)&D->obs, (size_t)D->N * obs_fields(D) * sizeof(double)))) return st;
     StepParams P;
     base_params(D, P, D->t);
     P.observe = 1;
@@ -1150,18 +1241,24 @@ struct Section {
 };
 
 // `t` selects the population buffers: the ones the step at time t reads.
+// Sections: populations; per scalar (at least one triple, empty without
+// scalars) its populations, adsorbed amount and previous value; the residual
+// moments; the face layers.
 std::vector<Section> ckpt_sections(const lbf_domain* D, long long t) {
     std::vector<Section> s;
     const size_t eb = st_bytes(D->st), rb = rt_bytes(D->st);
     s.push_back({D->pop[D->inplace ? 0 : (t & 1)], (size_t)D->q * D->Np * eb});
-    s.push_back({D->scalar ? D->gpop[t & 1] : nullptr, D->scalar ? (size_t)D->q * D->Np * rb : 0});
-    s.push_back({D->qads, D->qads ? (size_t)D->N * rb : 0});
-    s.push_back({D->cprev, D->cprev ? (size_t)D->N * rb : 0});
+    for (int si = 0; si < std::max(D->ns, 1); ++si) {
+        const bool has = si < D->ns;
+        s.push_back({has ? D->gpop[si][t & 1] : nullptr, has ? (size_t)D->q * D->Np * rb : 0});
+        s.push_back({D->qads[si], D->qads[si] ? (size_t)D->N * rb : 0});
+        s.push_back({D->cprev[si], D->cprev[si] ? (size_t)D->N * rb : 0});
+    }
     for (int k = 0; k < 2; ++k)
         s.push_back({D->mom[k], D->mom[k] ? (size_t)D->nfields() * D->N * rb : 0});
     for (int f = 0; f < 6; ++f)
         for (int k = 0; k < 2; ++k)
-            s.push_back({D->pb[f][k], D->pb[f][k] ? (size_t)2 * (D->d + 1) * D->pb_plane[f] * rb : 0});
+            s.push_back({D->pb[f][k], D->pb[f][k] ? (size_t)2 * D->pb_nf() * D->pb_plane[f] * rb : 0});
     return s;
 }
 
@@ -1264,9 +1361,7 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     }
     lbf_status st;
     D->Np = (N + 63) / 64 * 64;   // every plane starts on a 256-byte boundary
-    const size_t pbytes = (size_t)D->q * D->Np * st_bytes(D->st);
-    for (int k = 0; k < 2; ++k)
-        if ((st = dmalloc(D, &D->pop[k], pbytes))) { delete D; return st; }
+    // the population buffers are allocated once the layout is known (prepare)
     D->accum_cap = accum_slots(n, nf);
     if ((st = dmalloc(D, (void**)&D->accum, (size_t)ACCUM_PLANES * D->accum_cap * sizeof(double)))) { delete D; return st; }
     if ((st = dmalloc(D, (void**)&D->res_dev, 8 * sizeof(double)))) { delete D; return st; }
@@ -1284,8 +1379,8 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
 
 lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
     if (!D || !s) return fail(LBF_EINVAL, "null argument");
-    if (D->scalar) return fail(LBF_EINVAL, "one scalar per domain");
-    if (D->initialized || D->prepared) return fail(LBF_ESTATE, "attach the scalar before lbf_domain_init");
+    if (D->ns >= NSMAX) return fail(LBF_EUNSUPPORTED, "at most LBF_MAX_SCALARS scalars per domain");
+    if (D->initialized || D->prepared) return fail(LBF_ESTATE, "attach the scalars before lbf_domain_init");
     if (z_restricted(D)) return fail(LBF_EUNSUPPORTED, "z-slab domains with a scalar are not built");
     if (s->velocity_set != D->vs)
         return fail(LBF_EUNSUPPORTED, "on the device the scalar uses the momentum velocity set");
@@ -1304,26 +1399,30 @@ lbf_status lbf_scalar_attach(lbf_domain* D, const lbf_scalar_desc* s) {
         if (D->n[f / 2] < 4) return fail(LBF_EINVAL, "an extrapolation outflow face needs >= 4 nodes along its normal");
         outflow |= 1u << f;
     }
+    // the face pass serves the outflow faces of every scalar at once
+    const unsigned all = outflow | D->outflow;
     for (int f = 0; f < D->nfaces; ++f)
         for (int g = 0; g < D->nfaces; ++g)
-            if ((outflow >> f & 1u) && (outflow >> g & 1u) && f / 2 != g / 2)
+            if ((all >> f & 1u) && (all >> g & 1u) && f / 2 != g / 2)
                 return fail(LBF_EUNSUPPORTED, "extrapolation outflow on two faces that share an edge is not built");
-    D->outflow = outflow;
-    D->sdesc = *s;
-    D->sdesc.initial_scalar_field = nullptr;
-    if (s->initial_scalar_field) D->c0.assign(s->initial_scalar_field, s->initial_scalar_field + D->N);
+    const int si = D->ns;
     lbf_status st;
     const size_t rb = rt_bytes(D->st);
-    for (int k = 0; k < 2; ++k)
-        if ((st = dmalloc(D, &D->gpop[k], (size_t)D->q * D->Np * rb))) return st;
+    // the scalar populations are allocated with the momentum ones, once the layout is known
     if (s->has_adsorption) {
-        if ((st = dmalloc(D, &D->qads, D->N * rb))) return st;
-        if ((st = dmalloc(D, &D->cprev, D->N * rb))) return st;
+        if ((st = dmalloc(D, &D->qads[si], D->N * rb))) return st;
+        if ((st = dmalloc(D, &D->cprev[si], D->N * rb))) return st;
     }
-    if (!D->c0.empty()) {
-        if ((st = dmalloc(D, (void**)&D->c_init_dev, D->N * sizeof(double)))) return st;
-        CK(cudaMemcpy(D->c_init_dev, D->c0.data(), D->N * sizeof(double), cudaMemcpyHostToDevice));
+    if (s->initial_scalar_field) {
+        if ((st = dmalloc(D, (void**)&D->c_init_dev[si], D->N * sizeof(double)))) return st;
+        CK(cudaMemcpy(D->c_init_dev[si], s->initial_scalar_field, D->N * sizeof(double), cudaMemcpyHostToDevice));
+        D->c0[si].assign(s->initial_scalar_field, s->initial_scalar_field + D->N);
     }
+    D->outflow = all;
+    D->outflow_s[si] = outflow;
+    D->sdesc[si] = *s;
+    D->sdesc[si].initial_scalar_field = nullptr;
+    D->ns = si + 1;
     D->scalar = true;
     return LBF_OK;
 }
@@ -1368,7 +1467,7 @@ lbf_status lbf_domain_step_part(lbf_domain* D, int32_t part, int64_t k, void* st
         e = sweep_planes(D, P, z0 + 1, z1 - 1, s);
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
         if (P.residual) {
-            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, 5, 1, D->res_dev);
+            k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, D->nacc(), 1, D->res_dev);
             CK(cudaGetLastError());
             CK(cudaMemcpyAsync(D->res_host, D->res_dev, 8 * sizeof(double), cudaMemcpyDeviceToHost, s));
             D->res_step = t;
@@ -1395,7 +1494,7 @@ lbf_status lbf_domain_run(lbf_domain* D, int64_t max_iterations, int64_t k, doub
             CK(cudaStreamSynchronize(s));
             bool conv = D->res_host[0] <= tr;
             for (int a = 0; a < D->d; ++a) conv = conv && D->res_host[1 + a] <= tu;
-            if (D->scalar) conv = conv && D->res_host[4] <= tc;
+            for (int si = 0; si < D->ns; ++si) conv = conv && D->res_host[4 + si] <= tc;
             if (!std::isfinite(D->res_host[0])) return fail(LBF_ENAN, "non-finite residual");
             stop = conv;
         }
@@ -1411,28 +1510,52 @@ lbf_status lbf_domain_residuals(lbf_domain* D, double* out, int64_t* time_step) 
     CK(cudaStreamSynchronize(D->last_stream));
     lbf_status est = check_err(D);
     if (est) return est;
-    for (int k = 0; k < D->nfields(); ++k) out[k] = D->res_host[k];
-    if (D->scalar && D->d == 2) out[3] = D->res_host[4];
+    for (int k = 0; k < 1 + D->d; ++k) out[k] = D->res_host[k];
+    for (int si = 0; si < D->ns; ++si) out[1 + D->d + si] = D->res_host[4 + si];
     if (time_step) *time_step = D->res_step;
     return LBF_OK;
 }
+
+}  // extern "C"
+
+namespace {
+// Observed moments of f_t into D->obs; solid nodes keep their initial values
+// (they are never updated), filled on the device when those are uniform.
+// `uniform` tells whether the host still has to fill them.
+lbf_status observe_filled(lbf_domain* D, cudaStream_t s, bool& uniform) {
+    lbf_status st;
+    if ((st = do_observe(D, s))) return st;
+    const long long N = D->N;
+    uniform = D->rho0.empty() && D->u0.empty();
+    for (int si = 0; si < D->ns; ++si) uniform = uniform && D->c0[si].empty();
+    if (uniform && D->n_fluid < (unsigned long long)N) {
+        const unsigned nb = (unsigned)((N + 255) / 256);
+        for (int si = 0; si < std::max(D->ns, 1); ++si) {
+            // the first launch fills rho and u as well; the others are the same values again
+            k_fill_solid<<<nb, 256, 0, s>>>(D->dtype, N, D->d, D->obs, D->obs + N,
+                                            si < D->ns ? D->obs + N * (1 + D->d + si) : nullptr, D->rho0u, D->u0u[0],
+                                            D->u0u[1], D->u0u[2], si < D->ns ? D->sdesc[si].initial_scalar_value : 0.0);
+        }
+        CK(cudaGetLastError());
+    }
+    return LBF_OK;
+}
+
+double scalar_init_at(const lbf_domain* D, int si, long long i) {
+    return D->c0[si].empty() ? D->sdesc[si].initial_scalar_value : D->c0[si][(size_t)i];
+}
+}  // namespace
+
+extern "C" {
 
 lbf_status lbf_domain_get_moments(lbf_domain* D, double* rho, double* u, double* c, void* stream) {
     if (!D) return fail(LBF_EINVAL, "null domain");
     if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
     cudaStream_t s = (cudaStream_t)stream;
     lbf_status st;
-    if ((st = do_observe(D, s))) return st;
+    bool uniform = true;
+    if ((st = observe_filled(D, s, uniform))) return st;
     const long long N = D->N;
-    // solid nodes keep their initial values (they are never updated): filled on the
-    // device when those are uniform
-    const bool uniform = D->rho0.empty() && D->u0.empty() && (!D->scalar || D->c0.empty());
-    if (uniform && D->n_fluid < (unsigned long long)N) {
-        k_fill_solid<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(
-            D->dtype, N, D->d, D->obs, D->obs + N, D->scalar ? D->obs + N * (1 + D->d) : nullptr, D->rho0u,
-            D->u0u[0], D->u0u[1], D->u0u[2], D->scalar ? D->sdesc.initial_scalar_value : 0.0);
-        CK(cudaGetLastError());
-    }
     if (rho) CK(download(rho, D->obs, N * 8, s));
     if (u) CK(download(u, D->obs + N, N * D->d * 8, s));
     if (c && D->scalar) CK(download(c, D->obs + N * (1 + D->d), N * 8, s));
@@ -1443,27 +1566,49 @@ lbf_status lbf_domain_get_moments(lbf_domain* D, double* rho, double* u, double*
         if (!D->type[i]) continue;
         if (rho) rho[i] = D->rho0.empty() ? D->rho0u : D->rho0[i];
         if (u) for (int a = 0; a < D->d; ++a) u[i * D->d + a] = D->u0.empty() ? D->u0u[a] : D->u0[i * D->d + a];
-        if (c && D->scalar) c[i] = D->c0.empty() ? D->sdesc.initial_scalar_value : D->c0[i];
+        if (c && D->scalar) c[i] = scalar_init_at(D, 0, i);
     }
     return LBF_OK;
 }
 
-lbf_status lbf_domain_get_q_ads(lbf_domain* D, double* q) {
+lbf_status lbf_domain_get_scalar(lbf_domain* D, int32_t index, double* c, void* stream) {
+    if (!D || !c) return fail(LBF_EINVAL, "null argument");
+    if (index < 0 || index >= D->ns) return fail(LBF_EINVAL, "no scalar with that index");
+    if (D->batch) return fail(LBF_ESTATE, "the domain is in a batch (poll or evict it first)");
+    cudaStream_t s = (cudaStream_t)stream;
+    lbf_status st;
+    bool uniform = true;
+    if ((st = observe_filled(D, s, uniform))) return st;
+    const long long N = D->N;
+    CK(download(c, D->obs + N * (1 + D->d + index), N * 8, s));
+    CK(cudaStreamSynchronize(s));
+    if ((st = check_err(D))) return st;
+    if (!uniform)
+        for (long long i = 0; i < N; ++i)
+            if (D->type[i]) c[i] = scalar_init_at(D, index, i);
+    return LBF_OK;
+}
+
+lbf_status lbf_domain_get_q_ads_at(lbf_domain* D, int32_t index, double* q) {
     if (!D || !q) return fail(LBF_EINVAL, "null argument");
+    if (index < 0 || (index >= D->ns && !(index == 0 && D->ns == 0))) return fail(LBF_EINVAL, "no scalar with that index");
     CK(cudaStreamSynchronize(D->last_stream));
-    if (!D->qads) {
+    void* qa = D->qads[index];
+    if (!qa) {
         std::fill(q, q + D->N, 0.0);
         return LBF_OK;
     }
     if (D->st == LBF_STORE_F64) {
-        CK(cudaMemcpy(q, D->qads, D->N * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(q, qa, D->N * 8, cudaMemcpyDeviceToHost));
     } else {
         std::vector<float> tmp(D->N);
-        CK(cudaMemcpy(tmp.data(), D->qads, D->N * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tmp.data(), qa, D->N * 4, cudaMemcpyDeviceToHost));
         for (long long i = 0; i < D->N; ++i) q[i] = tmp[i];
     }
     return LBF_OK;
 }
+
+lbf_status lbf_domain_get_q_ads(lbf_domain* D, double* q) { return lbf_domain_get_q_ads_at(D, 0, q); }
 
 lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     if (!D || !out) return fail(LBF_EINVAL, "null argument");
@@ -1472,7 +1617,8 @@ lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     lbf_status st;
     if ((st = do_observe(D, s))) return st;
     const long long N = D->N;
-    const double* c = D->scalar ? D->obs + N * (1 + D->d) : nullptr;
+    const double* c = D->scalar ? D->obs + N * (1 + D->d) : nullptr;   // scalar 0
+    const void* qa0 = D->qads[0];
     // the swept planes only (all of them unless the domain is a z-slab)
     const long long o = zb(D) * D->n[0] * D->n[1], M = (ze(D) - zb(D)) * D->n[0] * D->n[1];
     const unsigned nb = (unsigned)((M + 255) / 256);
@@ -1480,11 +1626,11 @@ lbf_status lbf_domain_inventory(lbf_domain* D, double* out, void* stream) {
     const double* uu = D->obs + N + o * D->d;
     const double* cc = c ? c + o : nullptr;
     if (D->d == 2) {
-        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum, D->accum_cap);
-        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum, D->accum_cap);
+        if (D->st == LBF_STORE_F64) k_inventory<2, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, qa0 ? (const double*)qa0 + o : nullptr, D->accum, D->accum_cap);
+        else k_inventory<2, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, qa0 ? (const float*)qa0 + o : nullptr, D->accum, D->accum_cap);
     } else {
-        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const double*)D->qads + o : nullptr, D->accum, D->accum_cap);
-        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, D->qads ? (const float*)D->qads + o : nullptr, D->accum, D->accum_cap);
+        if (D->st == LBF_STORE_F64) k_inventory<3, double><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, qa0 ? (const double*)qa0 + o : nullptr, D->accum, D->accum_cap);
+        else k_inventory<3, float><<<nb, 256, 0, s>>>(D->mask + o, M, rho, uu, cc, qa0 ? (const float*)qa0 + o : nullptr, D->accum, D->accum_cap);
     }
     CK(cudaGetLastError());
     double* tmp = nullptr;
@@ -1623,7 +1769,7 @@ lbf_status lbf_domain_save(lbf_domain* D, void* host, int64_t cap, void* stream)
     std::memcpy(h.magic, "LBFCKPT1", 8);
     h.vs = D->vs; h.q = D->q; h.st = D->st; h.d = D->d;
     h.N = D->N; h.Np = D->Np; h.nlist = D->sparse ? D->nlist : 0;
-    h.sparse = D->sparse ? 1 : 0; h.scalar = D->scalar ? 1 : 0; h.ads = D->qads ? 1 : 0;
+    h.sparse = D->sparse ? 1 : 0; h.scalar = D->ns; h.ads = ads_bits(D);
     h.nsec = (int32_t)secs.size();
     h.t = D->t; h.res_step = D->res_step;
     for (int i = 0; i < 8; ++i) h.res[i] = D->res_host[i];
@@ -1649,8 +1795,8 @@ lbf_status lbf_domain_load(lbf_domain* D, const void* host, int64_t bytes, void*
     std::memcpy(&h, host, sizeof(h));
     if (std::memcmp(h.magic, "LBFCKPT1", 8) != 0) return fail(LBF_EINVAL, "not a checkpoint (bad magic)");
     if (h.vs != D->vs || h.q != D->q || h.st != D->st || h.N != D->N || h.Np != D->Np ||
-        h.sparse != (D->sparse ? 1 : 0) || (h.sparse && h.nlist != D->nlist) || h.scalar != (D->scalar ? 1 : 0) ||
-        h.ads != (D->qads ? 1 : 0))
+        h.sparse != (D->sparse ? 1 : 0) || (h.sparse && h.nlist != D->nlist) || h.scalar != D->ns ||
+        h.ads != ads_bits(D))
         return fail(LBF_EINVAL, "checkpoint of a different lattice, storage, layout or scalar set-up");
     if (h.t < 0 || h.res_step < -1 || h.res_step > h.t) return fail(LBF_EINVAL, "checkpoint time step out of range");
     // everything is validated before the domain changes: a rejected checkpoint

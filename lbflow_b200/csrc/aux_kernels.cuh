@@ -73,10 +73,11 @@ __global__ void k_setup(const SetupParams S) {
 }
 
 struct InitParams {
-    double rho0, u0[3], c0, q0;
-    const double* rho_field;   // or null
-    const double* u_field;     // [N][D] or null
-    const double* c_field;     // or null
+    double rho0, u0[3];
+    double c0[NSMAX], q0[NSMAX];       // per scalar: uniform initial value and adsorbed amount
+    const double* rho_field;           // or null
+    const double* u_field;             // [N][D] or null
+    const double* c_field[NSMAX];      // per scalar, or null
     int skip_pops;             // k_init: leave the populations (the sparse layout sets them by fluid slot)
     int pad;
 };
@@ -107,7 +108,6 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
     double u[3] = {I0.u0[0], I0.u0[1], I0.u0[2]};
     if (I0.u_field)
         for (int a = 0; a < D; ++a) u[a] = I0.u_field[cell * D + a];
-    const double c0 = I0.c_field ? I0.c_field[cell] : I0.c0;
     const uint32_t mk = P.mask[cell];
     const bool fluid = !(mk & M_SOLID);
     double uu = 0.0;
@@ -119,24 +119,26 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
             const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
             S::st(const_cast<void*>(P.srcp[i]), cell, S::sc(R(fe)));
         });
-        if constexpr (SCALAR) {
-            sfor<Q>([&](auto Ii) {
-                constexpr int i = Ii;
-                ((R*)P.gsrcp[i])[cell] = R(feq_i<L, double>(i, c0, u, uu));
-            });
-        }
+    }
+    if (fluid && P.mom_prev) {
+        R* mp = (R*)P.mom_prev;
+        mp[cell] = R(rho);
+        for (int a = 0; a < D; ++a) mp[(1 + a) * P.N + cell] = R(u[a]);
     }
     if constexpr (SCALAR) {
-        // every node, solid ones included: device memory comes uninitialised from the pool
-        if (P.qads) ((R*)P.qads)[cell] = (fluid && (mk & M_BB)) ? R(I0.q0) : R(0);
-        if (P.cprev) ((R*)P.cprev)[cell] = R(c0);
-    }
-    if (fluid) {
-        if (P.mom_prev) {
-            R* mp = (R*)P.mom_prev;
-            mp[cell] = R(rho);
-            for (int a = 0; a < D; ++a) mp[(1 + a) * P.N + cell] = R(u[a]);
-            if (SCALAR) mp[(1 + D) * P.N + cell] = R(c0);
+        for (int si = 0; si < P.nscalar; ++si) {
+            const ScalarParams& sc = P.sc[si];
+            const double c0 = I0.c_field[si] ? I0.c_field[si][cell] : I0.c0[si];
+            if (fluid && !I0.skip_pops) {
+                sfor<Q>([&](auto Ii) {
+                    constexpr int i = Ii;
+                    ((R*)sc.gsrc)[i * P.np + cell] = R(feq_i<L, double>(i, c0, u, uu));
+                });
+            }
+            // every node, solid ones included: device memory comes uninitialised from the pool
+            if (sc.qads) ((R*)sc.qads)[cell] = (fluid && (mk & M_BB)) ? R(I0.q0[si]) : R(0);
+            if (sc.cprev) ((R*)sc.cprev)[cell] = R(c0);
+            if (fluid && P.mom_prev) ((R*)P.mom_prev)[(1 + D + si) * P.N + cell] = R(c0);
         }
     }
     void* pbs[6][2] = {{pb0_0, pb0_1}, {pb1_0, pb1_1}, {pb2_0, pb2_1}, {pb3_0, pb3_1}, {pb4_0, pb4_1}, {pb5_0, pb5_1}};
@@ -147,8 +149,12 @@ __global__ void k_init(const StepParams P, const InitParams I0, void* pb0_0, voi
         const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
         for (int par = 0; par < 2; ++par) {
             R* pb = (R*)pbs[F][par];
-            for (int a = 0; a < D; ++a) pb[(dist * (D + 1) + a) * pl + pos] = R(u[a]);
-            pb[(dist * (D + 1) + D) * pl + pos] = R(c0);
+            for (int a = 0; a < D; ++a) pb[(dist * P.pb_nf + a) * pl + pos] = R(u[a]);
+            for (int si = 0; si < P.pb_nf - D; ++si) {
+                const double c0 = si < P.nscalar && I0.c_field[si] ? I0.c_field[si][cell]
+                                                                    : (si < P.nscalar ? I0.c0[si] : 0.0);
+                pb[(dist * P.pb_nf + D + si) * pl + pos] = R(c0);
+            }
         }
     }
 }
@@ -179,11 +185,11 @@ __global__ void k_init_sparse(const StepParams P, const InitParams I0) {
         const double fe = S::DEV ? heq_i<L, double>(i, rho, rho - 1.0, u, uu) : feq_i<L, double>(i, rho, u, uu);
         S::st(const_cast<void*>(P.srcp[i]), (int)k, S::sc(R(fe)));
     });
-    if (P.has_scalar) {   // g = g_eq(C0, u0) at the same slot (FP64 / FP32 storage only)
-        const double c0 = I0.c_field ? I0.c_field[cell] : I0.c0;
+    for (int si = 0; si < P.nscalar; ++si) {   // g = g_eq(C0, u0) at the same slot (FP64 / FP32 storage only)
+        const double c0 = I0.c_field[si] ? I0.c_field[si][cell] : I0.c0[si];
         sfor<Q>([&](auto Ii) {
             constexpr int i = Ii;
-            ((R*)P.gsrcp[i])[k] = R(feq_i<L, double>(i, c0, u, uu));
+            ((R*)P.sc[si].gsrc)[i * P.np + k] = R(feq_i<L, double>(i, c0, u, uu));
         });
     }
     if (P.mom_prev) {

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
                              lk ? g.cell : g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P));
             });
         }
-        process_cell<VS, COLL, ST, FACEBC, false>(P, g, mk, f, nullptr, racc);
+        process_cell<VS, COLL, ST, FACEBC, false>(P, g, mk, f, racc, NoScalarPull{});
     }
     if (!P.first) {
         // solid nodes sharing a 32-byte sector with a fluid node store zeros (full-sector stores)

@@ -71,6 +71,29 @@ struct SFaceBC {
     double u[3];
 };
 
+// Passive scalars per domain.  They share the momentum lattice (one momentum
+// sweep advances all of them, passive_scalar::LatticeVec) and nothing else.
+constexpr int NSMAX = 4;
+
+// One passive scalar (same velocity set as the momentum lattice).
+struct ScalarParams {
+    int coll, inner, has_source, ads;
+    double tau, omega, op, om, source;
+    double bgk_cb;           // 1 - 1/(2 tau) of the BGK source, computed once
+    double ka, kd, qmax;
+    double c_solid;          // initial scalar of solid nodes when uniform
+    const double* c_init;    // per-node initial scalar, or null
+    const void* gsrc;        // plane 0 of g*_{t-1} (g_0 when first); plane i at + i * np elements
+    void* gdst;              // plane 0 of g*_t
+    void* qads;              // adsorbed amount per node (compute type), in place
+    void* cprev;             // scalar value of the previous step per node, in place
+    // post-stream scalar populations of layers 1 and 2 inside each outflow face,
+    // written by the bulk sweep and read by the face pass of the same step:
+    // [layer 0/1][direction][plane node], compute type
+    void* snap[6];
+    SFaceBC face[6];
+};
+
 // The leading fields of a batch member's device state (BatchState): a single-
 // domain sweep launched inside a batch's chunk graph skips its launch when the
 // domain has stopped or the step (t0 + gate_j) is past its last one.
@@ -116,17 +139,13 @@ struct StepParams {
     unsigned tstep;           // time step of the launch (low 32 bits; the rounding seed)
     int tpad;
     long long seed_offset;    // node index of this lattice's node 0 in the whole lattice (z-slabs)
-    double bgk_cb, s_bgk_cb;  // 1 - 1/(2 tau) of the momentum and scalar BGK sources, computed once
-    // post-stream scalar populations of layers 1 and 2 inside each outflow face,
-    // written by the bulk sweep and read by the face pass of the same step:
-    // [layer 0/1][direction][plane node], compute type
-    void* snap[6];
+    double bgk_cb;            // 1 - 1/(2 tau) of the momentum BGK source, computed once
     // previous-step moments of the two node layers next to each face:
-    // [layer 0/1][field u_0..u_{D-1}, C][plane node], compute type
+    // [layer 0/1][field u_0..u_{D-1}, C_0..][plane node], compute type, pb_nf fields
     const void* pb_src[6];
     void* pb_dst[6];
     long long pb_plane[6];
-    // per-node moments for residuals: [field][N] (rho, u_0.., C), compute type
+    // per-node moments for residuals: [field][N] (rho, u_0.., C_0..), compute type
     const void* mom_prev;
     void* mom_cur;
     double* accum;   // residual partials: [accumulator][accum_stride] per-block slots
@@ -134,19 +153,11 @@ struct StepParams {
     long long res_slots;             // batches: slots a member's residual step fills
     double* obs_rho;
     double* obs_u;
-    double* obs_c;
-    // passive scalar (same velocity set as the momentum lattice)
-    int has_scalar, s_coll, s_inner, s_has_source;
-    double s_tau, s_omega, s_op, s_om, s_source;
-    int s_ads, s_pad0, s_pad1, s_pad2;
-    double ka, kd, qmax;
-    double c_solid;          // initial scalar of solid nodes when uniform
-    const double* c_init;    // per-node initial scalar, or null
-    const void* gsrcp[27];
-    void* gdstp[27];
-    void* qads;              // adsorbed amount per node (compute type), in place
-    void* cprev;             // scalar value of the previous step per node, in place
-    SFaceBC sface[6];
+    double* obs_c;           // scalar s at obs_c + s N
+    // passive scalars, advanced one after another in the momentum sweep
+    int has_scalar, nscalar;   // has_scalar = nscalar > 0
+    int pb_nf, ns_pad;         // fields per face layer: D + max(nscalar, 1)
+    ScalarParams sc[NSMAX];
 };
 
 template <int VS>
@@ -678,10 +689,11 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
         // wall velocity 1.5 u(x) - 0.5 u(x + n) from the previous step (bc.rs:86-117)
         const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
         const R* pb = (const R*)P.pb_src[F];
+        const int nf = P.pb_nf;
         R uw[3] = {R(0), R(0), R(0)};
 #pragma unroll
         for (int a = 0; a < L::D; ++a)
-            uw[a] = R(1.5) * pb[(0 * (L::D + 1) + a) * pl + pos] - R(0.5) * pb[(1 * (L::D + 1) + a) * pl + pos];
+            uw[a] = R(1.5) * pb[(0 * nf + a) * pl + pos] - R(0.5) * pb[(1 * nf + a) * pl + pos];
         R uu = R(0);
 #pragma unroll
         for (int a = 0; a < L::D; ++a) uu += uw[a] * uw[a];
@@ -704,19 +716,22 @@ __device__ __forceinline__ void momentum_face(const KParams<VS>& P, const Geo& g
     }
 }
 
-// Scalar face BCs (src/passive_scalar/bc.rs:37-152).  Extrapolation outflow
-// (zeroth / second order) is applied by the face pass.
+// Scalar face BCs of scalar `si` (src/passive_scalar/bc.rs:37-152).
+// Extrapolation outflow (zeroth / second order) is applied by the face pass.
 template <int VS, int F, class R>
-__device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, R* gg) {
+__device__ __forceinline__ void scalar_face(const KParams<VS>& P, int si, const Geo& g, R* gg) {
     using L = Lat<VS>;
-    const SFaceBC& b = P.sface[F];
+    const ScalarParams& sc = P.sc[si];
+    const SFaceBC& b = sc.face[F];
     const int kind = b.kind;
     if (kind == SBC_PERIODIC) return;
+    const R* gs = (const R*)sc.gsrc;
+    const long long np = P.np;
     if (kind == SBC_ZEROTH || kind == SBC_SECOND) {
         // extrapolation from the neighbours along the inward normal
         // (src/passive_scalar/bc.rs:154-199); only the face pass reaches here.
         const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
-        const R* sn = (const R*)P.snap[F];
+        const R* sn = (const R*)sc.snap[F];
         const bool second = kind == SBC_SECOND, all = !b.unknown_only;
         sfor<L::Q>([&](auto J) {
             constexpr int j = J;
@@ -730,13 +745,14 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
     if (kind == SBC_BB_NO_FLUX) {
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (leaves<L>(i, F)) gg[L::qbar(i)] = ((const R*)P.gsrcp[i])[g.slot];
+            if constexpr (leaves<L>(i, F)) gg[L::qbar(i)] = gs[i * np + g.slot];
         });
         return;
     }
     // anti-bounce-back with the wall equilibrium (bc.rs:107-140)
     const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
     const R* pb = (const R*)P.pb_src[F];
+    const int nf = P.pb_nf;
     R uw[3] = {R(0), R(0), R(0)};
     if (b.given_vel) {
 #pragma unroll
@@ -744,9 +760,9 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
     } else {
 #pragma unroll
         for (int a = 0; a < L::D; ++a)
-            uw[a] = R(1.5) * pb[(0 * (L::D + 1) + a) * pl + pos] - R(0.5) * pb[(1 * (L::D + 1) + a) * pl + pos];
+            uw[a] = R(1.5) * pb[(0 * nf + a) * pl + pos] - R(0.5) * pb[(1 * nf + a) * pl + pos];
     }
-    const R sval = kind == SBC_ANTI_BB ? R(b.value) : pb[(0 * (L::D + 1) + L::D) * pl + pos];
+    const R sval = kind == SBC_ANTI_BB ? R(b.value) : pb[(0 * nf + L::D + si) * pl + pos];
     R uu = R(0);
 #pragma unroll
     for (int a = 0; a < L::D; ++a) uu += uw[a] * uw[a];
@@ -757,37 +773,49 @@ __device__ __forceinline__ void scalar_face(const KParams<VS>& P, const Geo& g, 
 #pragma unroll
             for (int a = 0; a < L::D; ++a) cu += uw[a] * R(L::c(i, a));
             const R ge = R(L::w(i)) * sval * (R(1) + cu * R(3) + R(0.5) * cu * cu * R(9) - R(0.5) * uu * R(3));
-            gg[L::qbar(i)] = -((const R*)P.gsrcp[i])[g.slot] + R(2) * ge;
+            gg[L::qbar(i)] = -gs[i * np + g.slot] + R(2) * ge;
         }
     });
 }
 
-// Apply the face BCs of a node in the configured order (P.order).
-template <int VS, int ST, bool SCALAR>
-__device__ __forceinline__ void apply_faces(const KParams<VS>& P, const Geo& g, typename Store<ST>::R* f,
-                                            typename Store<ST>::R* gg) {
+// Apply the momentum face BCs of a node in the configured order (P.order).
+// Both loops are unrolled: six copies of the face rules, but no loop state live
+// across them (a runtime loop over the order positions needs more registers).
+// Only nodes on explicit faces run this code; no-slip walls fold into the link
+// bits, so in a duct or a packed bed the bulk of the lattice never fetches it.
+template <int VS, int ST>
+__device__ __forceinline__ void apply_faces(const KParams<VS>& P, const Geo& g, typename Store<ST>::R* f) {
     using L = Lat<VS>;
-    using R = typename Store<ST>::R;
+    sfor<L::NF>([&](auto O) {
+        const int fr = P.order[O];
+        sfor<L::NF>([&](auto FF) {
+            constexpr int F = FF;
+            if (fr == F && on_face(g, F, P)) momentum_face<VS, ST, F>(P, g, f);
+        });
+    });
+}
+
+// The face BCs of scalar si in the same order.  The momentum and scalar rules
+// touch disjoint populations and read no result of one another, so running all
+// momentum faces first changes nothing.
+template <int VS, class R>
+__device__ __forceinline__ void apply_scalar_faces(const KParams<VS>& P, int si, const Geo& g, R* gg) {
+    using L = Lat<VS>;
     sfor<L::NF>([&](auto O) {
         const int fr = P.order[O];
         sfor<L::NF>([&](auto FF) {
             constexpr int F = FF;
             if (fr == F) {
-                if constexpr (SCALAR) {
-                    // snapshot for an outflow face F, taken where F sits in the face order
-                    if (P.snap[F]) {
-                        const int dist = face_dist(g, F, P);
-                        if (dist == 1 || dist == 2) {
-                            R* sn = (R*)P.snap[F];
-                            const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
-                            sfor<L::Q>([&](auto J) { sn[((dist - 1) * L::Q + J) * pl + pos] = gg[J]; });
-                        }
+                // snapshot for an outflow face F, taken where F sits in the face order
+                R* sn = (R*)P.sc[si].snap[F];
+                if (sn) {
+                    const int dist = face_dist(g, F, P);
+                    if (dist == 1 || dist == 2) {
+                        const long long pl = P.pb_plane[F], pos = face_pos(g, F, P);
+                        sfor<L::Q>([&](auto J) { sn[((dist - 1) * L::Q + J) * pl + pos] = gg[J]; });
                     }
                 }
-                if (on_face(g, F, P)) {
-                    momentum_face<VS, ST, F>(P, g, f);
-                    if constexpr (SCALAR) scalar_face<VS, F, R>(P, g, gg);
-                }
+                if (on_face(g, F, P)) scalar_face<VS, F, R>(P, si, g, gg);
             }
         });
     });
@@ -796,10 +824,10 @@ __device__ __forceinline__ void apply_faces(const KParams<VS>& P, const Geo& g, 
 // Scalar source of one node (src/passive_scalar/node.rs:258-266 with
 // src/passive_scalar/adsorption.rs:50-92).  Updates q when `commit`.
 template <class R>
-__device__ __forceinline__ bool scalar_source(const StepParams& P, bool bb, R c_stored, R& q, bool commit, R& out) {
-    if (!P.s_ads) {
-        out = R(P.s_source);
-        return P.s_has_source != 0;
+__device__ __forceinline__ bool scalar_source(const ScalarParams& P, bool bb, R c_stored, R& q, bool commit, R& out) {
+    if (!P.ads) {
+        out = R(P.source);
+        return P.has_source != 0;
     }
     R ads = R(0);
     if (bb) {
@@ -812,7 +840,7 @@ __device__ __forceinline__ bool scalar_source(const StepParams& P, bool bb, R c_
             q = qn;
         }
     }
-    out = P.s_has_source ? R(P.s_source) + ads : ads;
+    out = P.has_source ? R(P.source) + ads : ads;
     return true;
 }
 
@@ -1156,25 +1184,32 @@ __device__ __forceinline__ bool gated_off(const StepParams& P) {
     return g.done_t >= 0 || g.t0 + P.gate_j > g.last_t;
 }
 
-// Everything a fluid node does after its populations were pulled: face BCs,
-// moments, residual/observe/face-layer outputs, collision + store, and the
-// scalar step.  Shared by every sweep.
-// `put` stores the post-collision populations (see collide_store).
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class Put>
-__device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo& g, uint32_t mk,
-                                                 typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                                 typename Store<ST>::R* gg, double (&racc)[5], Put&& put) {
+// Residual accumulators of a sweep: rho, u_0..u_2, then one per scalar.
+template <bool SCALAR>
+__host__ __device__ constexpr int racc_n() { return SCALAR ? 4 + NSMAX : 5; }
+
+// The momentum part of a fluid node after its populations were pulled: face
+// BCs, moments, residual/observe/face-layer outputs, collision + store.
+// `madd(J, v)` takes the node's squared residual term J (rho, u_0..) on
+// residual steps; `put` stores the post-collision populations (see
+// collide_store).  Returns the velocity (force-shifted) and its square, which
+// the scalars' equilibria use.
+template <int VS, int COLL, int ST, bool FACEBC, class MAdd, class Put>
+__device__ __forceinline__ void momentum_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                              typename Store<ST>::R (&f)[Lat<VS>::Q], MAdd&& madd, Put&& put,
+                                              typename Store<ST>::R (&u)[3], typename Store<ST>::R& uu) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
     constexpr int Q = L::Q, D = L::D;
     constexpr bool DEV = S::DEV;
+    const bool face_node = FACEBC && !P.first && (mk & (M_FACE | M_NEAR));
     // ---- face boundary conditions ------------------------------------------
     if constexpr (FACEBC) {
-        if (!P.first && (mk & (M_FACE | M_NEAR))) {
+        if (face_node) {
             // the face rules work on unscaled populations
             sfor<Q>([&](auto I) { f[I] = S::unsc(f[I]); });
-            apply_faces<VS, ST, SCALAR>(P, g, f, SCALAR ? gg : nullptr);
+            apply_faces<VS, ST>(P, g, f);
             sfor<Q>([&](auto I) { f[I] = S::sc(f[I]); });
         }
     }
@@ -1185,7 +1220,7 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
     drho = S::unsc(drho);
     const R rho = DEV ? R(1) + drho : drho;   // with h = f - w, sum h = rho - 1
     const R inv_rho = rcp_rn(rho);   // correctly rounded: the same value as 1 / rho
-    R u[3] = {R(0), R(0), R(0)};
+    u[0] = u[1] = u[2] = R(0);
     sfor<D>([&](auto A) {
         R s = R(0);
         sfor<Q>([&](auto I) {
@@ -1199,46 +1234,27 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
     const bool force = P.has_force != 0;
     if (force) sfor<D>([&](auto A) { u[A] += R(0.5) * F[A] * inv_rho; });
     const R dr = DEV ? drho : rho - R(1);
-
-    // ---- scalar value (src/passive_scalar/node.rs:272-279) --------------------
-    R cval = R(0), q = R(0), cst = R(0);
-    const bool bb = (mk & M_BB) != 0;
-    if constexpr (SCALAR) {
-        R s = R(0);
-        sfor<Q>([&](auto I) { s += gg[I]; });
-        if (P.s_ads && bb) {
-            q = ((const R*)P.qads)[g.cell];
-            cst = ((const R*)P.cprev)[g.cell];
-        }
-        R src;
-        if (scalar_source<R>(P, bb, cst, q, !P.observe, src)) s += R(0.5) * src;
-        cval = s;
-    }
+    uu = R(0);
+    sfor<D>([&](auto A) { uu += u[A] * u[A]; });
 
     if (P.observe) {
         P.obs_rho[g.cell] = double(rho);
         sfor<D>([&](auto A) { P.obs_u[(long long)g.cell * D + A] = double(u[A]); });
-        if constexpr (SCALAR) P.obs_c[g.cell] = double(cval);
     } else {
         // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
         if (P.residual) {
             const R* mp = (const R*)P.mom_prev;
             const double d0 = double(rho) - double(mp[g.cell]);
-            racc[0] += d0 * d0;
+            madd(IC<0>{}, d0 * d0);
             sfor<D>([&](auto A) {
                 const double du = double(u[A]) - double(mp[(1 + A) * P.N + g.cell]);
-                racc[1 + A] += du * du;
+                madd(IC<1 + int(A)>{}, du * du);
             });
-            if constexpr (SCALAR) {
-                const double dc = double(cval) - double(mp[(1 + D) * P.N + g.cell]);
-                racc[4] += dc * dc;
-            }
         }
         if (P.write_mom) {
             R* mc = (R*)P.mom_cur;
             mc[g.cell] = rho;
             sfor<D>([&](auto A) { mc[(1 + A) * P.N + g.cell] = u[A]; });
-            if constexpr (SCALAR) mc[(1 + D) * P.N + g.cell] = cval;
         }
         // ---- previous-step layers next to faces (anti-BB, extrapolation) ---------
         if constexpr (FACEBC) {
@@ -1250,8 +1266,7 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
                         if (dist <= 1) {
                             R* pb = (R*)P.pb_dst[Fc];
                             const long long pl = P.pb_plane[Fc], pos = face_pos(g, Fc, P);
-                            sfor<D>([&](auto A) { pb[(dist * (D + 1) + A) * pl + pos] = u[A]; });
-                            pb[(dist * (D + 1) + D) * pl + pos] = cval;
+                            sfor<D>([&](auto A) { pb[(dist * P.pb_nf + A) * pl + pos] = u[A]; });
                         }
                     }
                 });
@@ -1259,31 +1274,91 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
         }
 
         // ---- equilibrium + collision --------------------------------------------
-        R uu = R(0);
-        sfor<D>([&](auto A) { uu += u[A] * u[A]; });
         // the seed follows the node (index in the whole lattice), so every layout,
         // streaming scheme and z-slab split rounds a node's values alike
         const uint32_t nseed = (ST == ST_F16 || ST == ST_BF16)
                                    ? mix32((uint32_t)((long long)g.cell + P.seed_offset) ^ (P.tstep * 0x9e3779b9u))
                                    : 0u;
         collide_store<VS, COLL, ST>(P, f, rho, dr, u, uu, F, force, nseed, put);
+    }
+}
 
-        if constexpr (SCALAR) {
+// The scalars of a fluid node, one after another (src/passive_scalar/lattice.rs:
+// 241-297, node.rs:258-294), with the momentum velocity u of the same step.
+// `gpull(si, gg)` fills gg with the pulled populations of scalar si, inner rule
+// applied (the own populations on the first step).  They are pulled after the
+// momentum store, so one population set is live at a time.  `radd(si, v)`
+// takes the node's squared residual term of scalar si on residual steps.
+template <int VS, int ST, bool FACEBC, class GPull, class RAdd>
+__device__ __forceinline__ void scalar_cells(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                             const typename Store<ST>::R (&u)[3], typename Store<ST>::R uu,
+                                             GPull&& gpull, RAdd&& radd) {
+    using L = Lat<VS>;
+    using R = typename Store<ST>::R;
+    constexpr int Q = L::Q, D = L::D;
+    const bool face_node = FACEBC && !P.first && (mk & (M_FACE | M_NEAR));
+    const bool bb = (mk & M_BB) != 0;
+    {
+#pragma unroll 1
+        for (int si = 0; si < P.nscalar; ++si) {
+            const ScalarParams& sc = P.sc[si];
+            R gg[Q];
+            gpull(si, gg);
+            if constexpr (FACEBC) {
+                if (face_node) apply_scalar_faces<VS, R>(P, si, g, gg);
+            }
+            // scalar value (node.rs:272-279)
+            R q = R(0), cst = R(0);
+            R cval = R(0);
+            sfor<Q>([&](auto I) { cval += gg[I]; });
+            if (sc.ads && bb) {
+                q = ((const R*)sc.qads)[g.cell];
+                cst = ((const R*)sc.cprev)[g.cell];
+            }
+            {
+                R src;
+                if (scalar_source<R>(sc, bb, cst, q, !P.observe, src)) cval += R(0.5) * src;
+            }
+            if (P.observe) {
+                P.obs_c[(long long)si * P.N + g.cell] = double(cval);
+                continue;
+            }
+            if (P.residual) {
+                const R* mp = (const R*)P.mom_prev;
+                const double dc = double(cval) - double(mp[(1 + D + si) * P.N + g.cell]);
+                radd(si, dc * dc);
+            }
+            if (P.write_mom) ((R*)P.mom_cur)[(1 + D + si) * P.N + g.cell] = cval;
+            if constexpr (FACEBC) {
+                if (P.any_face) {
+                    sfor<L::NF>([&](auto FF) {
+                        constexpr int Fc = FF;
+                        if (P.pb_dst[Fc]) {
+                            const int dist = face_dist(g, Fc, P);
+                            if (dist <= 1) {
+                                R* pb = (R*)P.pb_dst[Fc];
+                                const long long pl = P.pb_plane[Fc], pos = face_pos(g, Fc, P);
+                                pb[(dist * P.pb_nf + D + si) * pl + pos] = cval;
+                            }
+                        }
+                    });
+                }
+            }
             // equilibrium with the momentum velocity, then collision (ps/lattice.rs:254-272)
             R ge[Q];
             sfor<Q>([&](auto I) { ge[I] = feq_i<L, R>(I, cval, u, uu); });
-            if (P.s_coll == COLL_BGK) {
-                const R w1 = R(P.s_omega), w0 = R(1) - R(P.s_omega);
+            if (sc.coll == COLL_BGK) {
+                const R w1 = R(sc.omega), w0 = R(1) - R(sc.omega);
                 R src;
-                const bool has = scalar_source<R>(P, bb, cval, q, true, src);
-                const R cb = R(P.s_bgk_cb);
+                const bool has = scalar_source<R>(sc, bb, cval, q, true, src);
+                const R cb = R(sc.bgk_cb);
                 sfor<Q>([&](auto I) {
                     R v = w0 * gg[I] + w1 * ge[I];
                     if (has) v += cb * R(L::w(I)) * src;
                     gg[I] = v;
                 });
             } else {   // TRT, no source (src/lib.rs:118-127)
-                const R wp = R(P.s_op), wm = R(P.s_om);
+                const R wp = R(sc.op), wm = R(sc.om);
                 R out[Q];
                 sfor<Q>([&](auto I) {
                     constexpr int i = I, ib = L::qbar(i);
@@ -1292,33 +1367,59 @@ __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo
                 });
                 sfor<Q>([&](auto I) { gg[I] = out[I]; });
             }
-            sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.slot] = gg[I]; });
-            if (P.s_ads && bb) {
-                ((R*)P.qads)[g.cell] = q;
-                ((R*)P.cprev)[g.cell] = cval;
+            R* gd = (R*)sc.gdst;
+            sfor<Q>([&](auto I) { gd[(long long)I * P.np + g.slot] = gg[I]; });
+            if (sc.ads && bb) {
+                ((R*)sc.qads)[g.cell] = q;
+                ((R*)sc.cprev)[g.cell] = cval;
             }
         }
     }
 }
 
+// Everything a fluid node does after its populations were pulled: the momentum
+// part, then the scalars.  Shared by every sweep.
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class Put, class GPull, int K>
+__device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo& g, uint32_t mk,
+                                                 typename Store<ST>::R (&f)[Lat<VS>::Q], double (&racc)[K],
+                                                 Put&& put, GPull&& gpull) {
+    using R = typename Store<ST>::R;
+    R u[3], uu;
+    momentum_cell<VS, COLL, ST, FACEBC>(P, g, mk, f, [&](auto J, double v) { racc[int(J)] += v; }, put, u, uu);
+    if constexpr (SCALAR) {
+        // a static index keeps racc in registers
+        auto radd = [&](int si, double v) {
+            sfor<NSMAX>([&](auto J) {
+                if (si == int(J)) racc[4 + J] += v;
+            });
+        };
+        scalar_cells<VS, ST, FACEBC>(P, g, mk, u, uu, gpull, radd);
+    }
+}
+
+// A gpull for kernels without scalars.
+struct NoScalarPull {
+    template <class R>
+    __device__ __forceinline__ void operator()(int, R*) const {}
+};
+
 // The A/B layouts: the post-collision populations go to slot `pidx` of the
 // destination planes (the node index for the dense layouts, the fluid-node index
 // for the sparse layout).
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class GPull, int K>
 __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo& g, uint32_t mk,
-                                                typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                                typename Store<ST>::R* gg, double (&racc)[5], long long pidx) {
+                                                typename Store<ST>::R (&f)[Lat<VS>::Q], double (&racc)[K],
+                                                long long pidx, GPull&& gpull) {
     using S = Store<ST>;
-    process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc, [&](auto I, typename S::T v) {
-        ((typename S::T*)P.dstp[I])[pidx] = v;
-    });
+    process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(
+        P, g, mk, f, racc, [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[pidx] = v; }, gpull);
 }
 
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class GPull, int K>
 __device__ __forceinline__ void process_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
-                                             typename Store<ST>::R (&f)[Lat<VS>::Q],
-                                             typename Store<ST>::R* gg, double (&racc)[5]) {
-    process_cell_at<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc, g.cell);
+                                             typename Store<ST>::R (&f)[Lat<VS>::Q], double (&racc)[K],
+                                             GPull&& gpull) {
+    process_cell_at<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, racc, g.cell, gpull);
 }
 
 // =================================================================== the step
@@ -1393,7 +1494,8 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
                     const int zs = D == 3 ? (L::c(i, 2) > 0 ? g.zm : (L::c(i, 2) < 0 ? g.zp : g.z)) : 0;
                     const long long row = (long long)P.nx * ((long long)ys + (long long)P.ny * zs);
                     bulk_g2s(rows + (size_t)i * P.nx, (const T*)P.srcp[i] + row, rb, bar);
-                    if constexpr (SCALAR) bulk_g2s(grows + (size_t)i * P.nx, (const R*)P.gsrcp[i] + row, grb, bar);
+                    if constexpr (SCALAR)
+                        bulk_g2s(grows + (size_t)i * P.nx, (const R*)P.sc[0].gsrc + (size_t)i * P.np + row, grb, bar);
                 });
             }
             if (!mbar_wait_bounded(bar, 0, wait_limit(P))) {
@@ -1408,7 +1510,7 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
     bool active = !(mk & M_SOLID);
     if constexpr (FACEBC) active = active && ((P.face_pass != 0) == ((mk & M_SKIP) != 0));
 
-    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    double racc[racc_n<SCALAR>()] = {};
     if (active) {
         // ---- stream (pull) + inner bounce-back -------------------------------
         R f[Q];
@@ -1443,33 +1545,36 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
                 });
             }
         }
-        // scalar populations: pull + inner BC (src/passive_scalar/lattice.rs:274-297)
-        R gg[SCALAR ? Q : 1];
-        if constexpr (SCALAR) {
+        // scalar populations: pull + inner BC (src/passive_scalar/lattice.rs:274-297);
+        // the staged rows hold scalar 0
+        auto gpull = [&](int si, R* gg) {
+            const ScalarParams& sc = P.sc[si];
+            const R* gs = (const R*)sc.gsrc;
+            const long long np = P.np;
             if (P.first) {
-                sfor<Q>([&](auto I) { gg[I] = ((const R*)P.gsrcp[I])[g.cell]; });
-            } else {
-                sfor<Q>([&](auto I) {
-                    constexpr int i = I, ib = L::qbar(i);
-                    const int n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
-                    if (mk >> ib & 1u) {
-                        const R own = ((const R*)P.gsrcp[ib])[g.cell];
-                        if (P.s_inner == 1) {
-                            gg[i] = own;   // InnerBounceBack
-                        } else {           // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
-                            const R cs = P.c_init ? R(P.c_init[n]) : R(P.c_solid);
-                            gg[i] = -own + R(2) * R(L::w(ib)) * cs;
-                        }
-                    } else if (STAGE && staged) {
-                        const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
-                        gg[i] = grows[(size_t)i * P.nx + xs];
-                    } else {
-                        gg[i] = ((const R*)P.gsrcp[i])[n];
-                    }
-                });
+                sfor<Q>([&](auto I) { gg[I] = gs[I * np + g.cell]; });
+                return;
             }
-        }
-        process_cell<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc);
+            sfor<Q>([&](auto I) {
+                constexpr int i = I, ib = L::qbar(i);
+                const int n = g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P);
+                if (mk >> ib & 1u) {
+                    const R own = gs[ib * np + g.cell];
+                    if (sc.inner == 1) {
+                        gg[i] = own;   // InnerBounceBack
+                    } else {           // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
+                        const R cs = sc.c_init ? R(sc.c_init[n]) : R(sc.c_solid);
+                        gg[i] = -own + R(2) * R(L::w(ib)) * cs;
+                    }
+                } else if (STAGE && staged && si == 0) {
+                    const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
+                    gg[i] = grows[(size_t)i * P.nx + xs];
+                } else {
+                    gg[i] = gs[i * np + n];
+                }
+            });
+        };
+        process_cell<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, racc, gpull);
     }
     if (!P.observe && !P.face_pass && !P.first) {
         // Solid nodes are never read, but storing them when a node in the same
@@ -1481,10 +1586,14 @@ __global__ void __launch_bounds__(STAGE ? 512 : 256, (STAGE ? 1 : 2) * light_ker
         const unsigned grp = (per >= 32 ? 0xffffffffu : ((1u << per) - 1u) << ((lane / per) * per));
         if (inside && (mk & M_SOLID) && (fl & grp)) {
             sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
-            if constexpr (SCALAR) sfor<Q>([&](auto I) { ((R*)P.gdstp[I])[g.cell] = R(0); });
+            if constexpr (SCALAR) {
+#pragma unroll 1
+                for (int si = 0; si < P.nscalar; ++si)
+                    sfor<Q>([&](auto I) { ((R*)P.sc[si].gdst)[I * P.np + g.cell] = R(0); });
+            }
         }
     }
-    if (P.residual && !P.observe) step_partials<5>(racc, P, block_linear());
+    if (P.residual && !P.observe) step_partials<racc_n<SCALAR>()>(racc, P, block_linear());
 }
 
 // =================================================================== compacted sweep
@@ -1558,7 +1667,7 @@ __global__ void __launch_bounds__(256, ST == ST_F64 ? 2 : 4) k_step_list(const K
                              lk ? g.cell : g.at(-L::c(i, 0), -L::c(i, 1), D == 3 ? -L::c(i, 2) : 0, P));
             });
         }
-        process_cell<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc);
+        process_cell<VS, COLL, ST, false, false>(P, g, mk, f, racc, NoScalarPull{});
     } else if (valid) {
         sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
     }
@@ -1692,7 +1801,7 @@ __global__ void __launch_bounds__(288, 3) k_step_pipe(const KParams<VS> P) {
                             f[i] = S::cvt(*p);
                         });
                     }
-                    process_cell<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc);
+                    process_cell<VS, COLL, ST, false, false>(P, g, mk, f, racc, NoScalarPull{});
                 }
                 constexpr int per = 32 / (int)sizeof(T);
                 const unsigned fl = __ballot_sync(0xffffffffu, active);
@@ -1793,7 +1902,7 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
     using S = Store<ST>;
     using R = typename S::R;
     using T = typename S::T;
-    constexpr int Q = L::Q, D = L::D;
+    constexpr int Q = L::Q;
     const bool valid = k64 < P.nlist;
     const int k = valid ? (int)k64 : (int)(P.nlist - 1);
     // an in-place even step reads the node's own slots: coordinates only for outputs
@@ -1838,13 +1947,13 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
     };
     if constexpr (MODE == SWEEP_AA_EVEN) {
         sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
-        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
+        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, racc, [&](auto I, T v) {
             ((T*)P.dstp[L::qbar(I)])[k] = v;
-        });
+        }, NoScalarPull{});
     } else if constexpr (MODE == SWEEP_PUSH) {
         sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
         auto body = [&](auto WRAP) {
-            process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
+            process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, racc, [&](auto I, T v) {
                 constexpr int i = I, ib = L::qbar(i);
                 if constexpr (i == 0) {
                     ((T*)P.dstp[0])[k] = v;
@@ -1854,7 +1963,7 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
                     const int idx = sparse_source<L, ib, decltype(WRAP)::value != 0>(P, g, k);
                     ((T*)(lk ? P.dstp[ib] : P.dstp[i]))[lk ? k : idx] = v;
                 }
-            });
+            }, NoScalarPull{});
         };
         if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) body(IC<1>{});
         else body(IC<0>{});
@@ -1877,9 +1986,9 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
         };
         if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) load(IC<1>{});
         else load(IC<0>{});
-        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, [&](auto I, T v) {
+        process_cell_put<VS, COLL, ST, false, false>(P, g, mk, f, racc, [&](auto I, T v) {
             ((T*)P.dstp[0])[off[L::qbar(I)]] = v;
-        });
+        }, NoScalarPull{});
     } else {
         if (P.first) {
             sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
@@ -1900,7 +2009,7 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
             if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
             else pull(IC<0>{});
         }
-        process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, nullptr, racc, k);
+        process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, racc, k, NoScalarPull{});
     }
 }
 
@@ -1979,22 +2088,28 @@ __global__ void __launch_bounds__(256, (sparse_blocks<VS, COLL, ST, MODE>())) k_
 // finds a node's fluid slot through the row words.  Per-node side arrays
 // (adsorbed amount, previous scalar value, residual moments, face layers) stay
 // indexed by node, as in the dense layout.
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
-__global__ void __launch_bounds__(256, 2) k_step_sparse_fs(const KParams<VS> P) {
-    using L = Lat<VS>;
-    using S = Store<ST>;
-    using R = typename S::R;
-    constexpr int Q = L::Q, D = L::D;
-    if (gated_off(P)) return;
-    Geo g;
-    uint32_t mk = M_SOLID;
+// Blocks per SM (ptxas, D3Q19 / D2Q9 BGK and TRT): the FP32 and 16-bit sweeps,
+// with or without scalars, fit 80 registers (three blocks); FP64, D3Q27 and MRT
+// keep 128 (two), below which they spill.  The scalars' pull reuses the
+// momentum's source slots from shared memory, and their residual terms wait
+// there for the block reduction, so neither is held in registers across the
+// momentum collision.
+template <int VS, int COLL, int ST, bool SCALAR>
+constexpr int sparse_fs_blocks() {
+    return (ST == ST_F64 || VS == VS_D3Q27 || COLL == COLL_MRT) ? 2 : 3;
+}
+
+// The node of thread `tid` in a launch of k_step_sparse_fs: its coordinates,
+// fluid slot k and mask word (face pass: the tid-th position of face fp_face).
+template <bool FACEBC>
+__device__ __forceinline__ bool sparse_fs_node(const StepParams& P, long long tid, Geo& g, int& k, uint32_t& mk) {
     bool valid;
-    int k = 0;
+    mk = M_SOLID;
+    k = 0;
     if (FACEBC && P.face_pass) {
         const int F = P.fp_face;
-        const long long pos = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-        valid = pos < P.pb_plane[F];
-        const long long pp = valid ? pos : 0;
+        valid = tid < P.pb_plane[F];
+        const long long pp = valid ? tid : 0;
         if (F < 2) { g.x = F == 0 ? 0 : P.nx - 1; g.y = (int)(pp % P.ny); g.z = (int)(pp / P.ny); }
         else if (F < 4) { g.y = F == 2 ? 0 : P.ny - 1; g.x = (int)(pp % P.nx); g.z = (int)(pp / P.nx); }
         else { g.z = F == 4 ? 0 : P.nz - 1; g.x = (int)(pp % P.nx); g.y = (int)(pp / P.nx); }
@@ -2006,7 +2121,7 @@ __global__ void __launch_bounds__(256, 2) k_step_sparse_fs(const KParams<VS> P) 
             k = (int)v.y + __popc(v.x & ((1u << (g.x & 31)) - 1u));
         }
     } else {
-        const long long k64 = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+        const long long k64 = P.kbeg + tid;
         valid = k64 < P.kend;
         k = valid ? (int)k64 : (int)(P.kend - 1);
         const uint32_t e = P.list[k];
@@ -2038,50 +2153,106 @@ __global__ void __launch_bounds__(256, 2) k_step_sparse_fs(const KParams<VS> P) 
     g.yp = g.y == P.ny - 1 ? 0 : g.y + 1;
     g.zm = g.z == 0 ? P.nz - 1 : g.z - 1;
     g.zp = g.z == P.nz - 1 ? 0 : g.z + 1;
-    double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    return valid;
+}
+
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR>
+__global__ void __launch_bounds__(256, (sparse_fs_blocks<VS, COLL, ST, SCALAR>())) k_step_sparse_fs(const KParams<VS> P) {
+    using L = Lat<VS>;
+    using S = Store<ST>;
+    using R = typename S::R;
+    constexpr int Q = L::Q, D = L::D;
+    // the pull's source slots for the scalars, [direction][thread]: the fluid slot,
+    // or ~k for a linked direction (the node's own slot k of plane ibar)
+    __shared__ int sidx[SCALAR ? Q * 256 : 1];
+    // with scalars, the squared residual terms of this block's nodes,
+    // [rho, u_0..u_2, scalar 0..][thread], kept out of registers until the block
+    // reduction
+    __shared__ double sres[SCALAR ? (4 + NSMAX) * 256 : 1];
+    if (gated_off(P)) return;
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int t = threadIdx.x;
+    Geo g;
+    uint32_t mk;
+    int k;
+    const bool valid = sparse_fs_node<FACEBC>(P, tid, g, k, mk);
+    double racc[5] = {};
     if (valid) {
         R f[Q];
-        R gg[SCALAR ? Q : 1];
+        R u[3], uu;
         if (P.first) {
             sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
-            if constexpr (SCALAR) sfor<Q>([&](auto I) { gg[I] = ((const R*)P.gsrcp[I])[k]; });
         } else {
-            // pull + inner bounce-back (src/lib.rs:141-165); the scalar's inner BC
-            // (src/passive_scalar/lattice.rs:274-297) on the same source index
+            // pull + inner bounce-back (src/lib.rs:141-165)
             auto pull = [&](auto WRAP) {
                 sfor<Q>([&](auto I) {
                     constexpr int i = I, ib = L::qbar(i);
                     const int idx = sparse_source<L, i, decltype(WRAP)::value != 0>(P, g, k);
                     const bool lk = (mk >> ib) & 1u;
                     f[i] = S::ld(lk ? P.srcp[ib] : P.srcp[i], lk ? k : idx);
-                    if constexpr (SCALAR) {
-                        if (lk) {
-                            const R own = ((const R*)P.gsrcp[ib])[k];
-                            if (P.s_inner == 1) {
-                                gg[i] = own;   // InnerBounceBack
-                            } else {           // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
-                                R cs = R(P.c_solid);
-                                if (P.c_init) {   // the solid neighbour's initial value (periodic)
-                                    const int xs = L::c(i, 0) > 0 ? g.xm : (L::c(i, 0) < 0 ? g.xp : g.x);
-                                    const int ys = L::c(i, 1) > 0 ? g.ym : (L::c(i, 1) < 0 ? g.yp : g.y);
-                                    const int zs = D == 3 ? (L::c(i, 2) > 0 ? g.zm : (L::c(i, 2) < 0 ? g.zp : g.z)) : 0;
-                                    cs = R(P.c_init[xs + (long long)P.nx * (ys + (long long)P.ny * zs)]);
-                                }
-                                gg[i] = -own + R(2) * R(L::w(ib)) * cs;
-                            }
-                        } else {
-                            gg[i] = ((const R*)P.gsrcp[i])[idx];
-                        }
-                    }
+                    if constexpr (SCALAR) sidx[i * 256 + t] = lk ? ~k : idx;
                 });
             };
+            // a lane of the warp at a row end: the periodic-wrap form of the source index
             if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
             else pull(IC<0>{});
         }
-        process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(P, g, mk, f, gg, racc,
-                                                        [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[k] = v; });
+        auto put = [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[k] = v; };
+        if constexpr (SCALAR) momentum_cell<VS, COLL, ST, FACEBC>(
+            P, g, mk, f, [&](auto J, double v) { sres[int(J) * 256 + t] = v; }, put, u, uu);
+        else momentum_cell<VS, COLL, ST, FACEBC>(P, g, mk, f, [&](auto J, double v) { racc[int(J)] += v; }, put, u, uu);
+        if constexpr (SCALAR) {
+            // the scalars: the momentum's source slots (a linked direction reads the
+            // node's own g*[ib]) and inner BC (src/passive_scalar/lattice.rs:274-297).
+            // The node's coordinates are taken again, so none stay live across the
+            // momentum collision.
+            Geo gq;
+            int kq;
+            uint32_t mq;
+            sparse_fs_node<FACEBC>(P, tid, gq, kq, mq);
+            auto gpull = [&](int si, R* gg) {
+                const ScalarParams& sc = P.sc[si];
+                const R* gs = (const R*)sc.gsrc;
+                const long long np = P.np;
+                if (P.first) {
+                    sfor<Q>([&](auto I) { gg[I] = gs[I * np + kq]; });
+                    return;
+                }
+                sfor<Q>([&](auto I) {
+                    constexpr int i = I, ib = L::qbar(i);
+                    const int e = sidx[i * 256 + t];
+                    const bool lk = e < 0;
+                    const R v = gs[(lk ? ib : i) * np + (lk ? ~e : e)];
+                    if (lk && sc.inner != 1) {   // InnerAntiBounceBack: -g*[ib] + 2 w C_solid (ps/node.rs:281-294)
+                        R cs = R(sc.c_solid);
+                        if (sc.c_init) {   // the solid neighbour's initial value (periodic)
+                            const int xs = L::c(i, 0) > 0 ? gq.xm : (L::c(i, 0) < 0 ? gq.xp : gq.x);
+                            const int ys = L::c(i, 1) > 0 ? gq.ym : (L::c(i, 1) < 0 ? gq.yp : gq.y);
+                            const int zs = D == 3 ? (L::c(i, 2) > 0 ? gq.zm : (L::c(i, 2) < 0 ? gq.zp : gq.z)) : 0;
+                            cs = R(sc.c_init[xs + (long long)P.nx * (ys + (long long)P.ny * zs)]);
+                        }
+                        gg[i] = -v + R(2) * R(L::w(ib)) * cs;
+                    } else {
+                        gg[i] = v;   // pulled, or InnerBounceBack
+                    }
+                });
+            };
+            scalar_cells<VS, ST, FACEBC>(P, gq, mq, u, uu, gpull,
+                                         [&](int si, double v) { sres[(4 + si) * 256 + t] = v; });
+        }
     }
-    if (P.residual && !P.observe) step_partials<5>(racc, P, blockIdx.x);
+    if (P.residual && !P.observe) {
+        if constexpr (SCALAR) {
+            double rall[4 + NSMAX];
+            sfor<4 + NSMAX>([&](auto J) {
+                const bool has = valid && (int(J) < 1 + D || (int(J) >= 4 && int(J) < 4 + P.nscalar));
+                rall[J] = has ? sres[int(J) * 256 + t] : 0.0;
+            });
+            step_partials<4 + NSMAX>(rall, P, blockIdx.x);
+        } else {
+            step_partials<5>(racc, P, blockIdx.x);
+        }
+    }
 }
 
 // =================================================================== z-slab halos

@@ -9,7 +9,7 @@ creating a Domain loads liblbflow_b200.so or raises.
 from __future__ import annotations
 
 import ctypes as C
-from typing import Optional
+from typing import Optional, Sequence, Union
 
 import numpy as np
 
@@ -33,7 +33,16 @@ def _stream_handle(stream) -> Optional[int]:
 
 
 class Domain:
-    def __init__(self, params: _m.Parameters, scalar: Optional[_ps.Parameters] = None,
+    """One lattice with up to LBF_MAX_SCALARS passive scalars.
+
+    `scalar` is one passive_scalar.Parameters or a sequence of them (the
+    reference's LatticeVec, src/passive_scalar/lattice.rs:353-430): one momentum
+    sweep advances every scalar.  moments() reports scalar 0; scalar(i) and
+    q_ads(i) the others; residuals() lists rho, u_a.., then every scalar.
+    """
+
+    def __init__(self, params: _m.Parameters,
+                 scalar: Union[None, _ps.Parameters, Sequence[_ps.Parameters]] = None,
                  desc: Optional[_abi.DomainDesc] = None, scalar_desc: Optional[_abi.ScalarDesc] = None):
         self.lib = _abi.load()
         keep = []
@@ -49,14 +58,22 @@ class Domain:
         self.h = h
         self.has_scalar = False
         self.scalar_name = None
+        self.scalar_names = []
+        scalars = [] if scalar is None else (list(scalar) if isinstance(scalar, (list, tuple)) else [scalar])
+        if len(scalars) > _abi.LBF_MAX_SCALARS:
+            self.close()
+            raise ValueError(f"at most {_abi.LBF_MAX_SCALARS} scalars per domain")
         try:
-            if scalar is not None or scalar_desc is not None:
-                if scalar_desc is None:
-                    scalar_desc, k2 = _ps.to_desc(scalar, self.n)
-                    keep += k2
-                    self.scalar_name = scalar.scalar_name
+            if scalar_desc is not None:
                 _abi.check(self.lib.lbf_scalar_attach(self.h, C.byref(scalar_desc)))
-                self.has_scalar = True
+                self.scalar_names.append(None)
+            for sp in scalars:
+                sd, k2 = _ps.to_desc(sp, self.n)
+                keep += k2
+                _abi.check(self.lib.lbf_scalar_attach(self.h, C.byref(sd)))
+                self.scalar_names.append(sp.scalar_name)
+            self.has_scalar = len(self.scalar_names) > 0
+            self.scalar_name = self.scalar_names[0] if self.has_scalar else None
         except Exception:
             self.close()
             raise
@@ -117,11 +134,16 @@ class Domain:
         _abi.check(self.lib.lbf_domain_device_bytes(self.h, C.byref(b)))
         return b.value
 
+    @property
+    def num_scalars(self) -> int:
+        return len(self.scalar_names)
+
     def residuals(self):
-        out = np.zeros(8)
+        """([rho, u_a.., scalar_0, ..], time step they belong to)."""
+        out = np.zeros(1 + 3 + _abi.LBF_MAX_SCALARS)
         t = C.c_int64()
         _abi.check(self.lib.lbf_domain_residuals(self.h, _ptr(out), C.byref(t)))
-        return out[: 1 + self.d + (1 if self.has_scalar else 0)], t.value
+        return out[: 1 + self.d + self.num_scalars], t.value
 
     def moments(self, stream=None):
         """(density[N], velocity[N, D], scalar[N] or None) at the current time step."""
@@ -131,9 +153,15 @@ class Domain:
         _abi.check(self.lib.lbf_domain_get_moments(self.h, _ptr(rho), _ptr(u), _ptr(c), _stream_handle(stream)))
         return rho, u.reshape(self.N, self.d), c
 
-    def q_ads(self):
+    def scalar(self, index: int = 0, stream=None) -> np.ndarray:
+        """Scalar `index` (attach order) at the current time step, [N]."""
         out = np.zeros(self.N)
-        _abi.check(self.lib.lbf_domain_get_q_ads(self.h, _ptr(out)))
+        _abi.check(self.lib.lbf_domain_get_scalar(self.h, int(index), _ptr(out), _stream_handle(stream)))
+        return out
+
+    def q_ads(self, index: int = 0):
+        out = np.zeros(self.N)
+        _abi.check(self.lib.lbf_domain_get_q_ads_at(self.h, int(index), _ptr(out)))
         return out
 
     def inventory(self, stream=None):

@@ -232,13 +232,15 @@ class _Arrivals:
 
 def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
                 residual_interval: int = 50, budget_bytes: int = 0, large_nodes: int = 1 << 19,
-                create_ms: float = 5.0, keep: Optional[set] = None) -> List[Record]:
+                create_ms: float = 5.0, keep: Optional[set] = None, large_slots: int = 1) -> List[Record]:
     """Run the requests through two batches ("lanes") that advance independently.
 
     Small requests (fewer than `large_nodes` nodes) go to a lane on a high-priority
     CUDA stream: its chunks hold only small domains, so they are short, and when
     SMs free up the scheduler runs its blocks ahead of the other lane's.  Large
-    requests go to a lane on a normal-priority stream.  Each lane runs one chunk
+    requests go to a lane on a normal-priority stream, at most `large_slots` at a
+    time (a large request fills the GPU alone; sharing it between several only
+    delays all of them, which sets the tail latency).  Each lane runs one chunk
     at a time; the host polls both without blocking, admits new members at chunk
     boundaries and, between polls, builds the domains of arrived requests,
     smallest first, while the device-memory budget allows.  The stop rule, the
@@ -288,6 +290,10 @@ def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float 
             arrivals.arrive(_now(t0))
             built = 0
             while arrivals.peek() is not None and used + arrivals.peek().est_bytes <= budget:
+                # smallest first: once the next one is large and the large lane has one
+                # waiting, the rest wait too (they are no smaller)
+                if lane_of(arrivals.peek(), large_nodes) == 1 and len(lanes[1]["ready"]) >= large_slots:
+                    break
                 r = arrivals.pop()
                 dom = Domain(r.params)
                 dom.init(s_init)
@@ -309,11 +315,12 @@ def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float 
                         futures.append(pool.submit(collect, r, dom, start, status, t0))
                         used -= r.est_bytes
                     ln["ev"] = None
-                for r, dom in ln["ready"]:
+                cap = large_slots if li == 1 else len(ln["ready"]) + len(ln["live"])
+                while ln["ready"] and len(ln["live"]) < cap:
+                    r, dom = ln["ready"].pop(0)
                     ln["batch"].admit(dom, max_it, tol_density=math.inf, tol_velocity=tol_velocity,
                                       tol_scalar=math.inf)
                     ln["live"][dom.h.value] = (r, dom, _now(t0))
-                ln["ready"].clear()
                 if ln["live"]:
                     ln["batch"].step(1, ln["stream"])
                     ln["ev"] = torch.cuda.Event()

@@ -24,9 +24,10 @@ default 100), `max_iterations` (--max-iterations, default 100000) and
 reference's parallel writer produces).  `freeze_momentum` is not supported by the
 fused kernel (it always advances momentum) and raises.
 
-Several scalars (`run_vec`) run as one engine domain per scalar: each advances
-the same momentum field (identical arithmetic, so identical values) plus its own
-scalar; momentum outputs and residuals come from the first.
+Several scalars (`run_vec`, passive_scalar::LatticeVec) are attached to one
+engine domain: each step advances the momentum populations once and every
+scalar after them in the same sweep, as the reference advances one momentum
+lattice and then each scalar lattice (src/passive_scalar.rs:136-177).
 """
 from __future__ import annotations
 
@@ -148,11 +149,10 @@ def solve(momentum_params: _m.Parameters, passive_scalar_params: Optional[Sequen
     paths = _case_directories(case_dir)
     wall0 = time.perf_counter()
 
-    doms = [Domain(momentum_params, s) for s in scalars] if scalars else [Domain(momentum_params)]
+    dom0 = Domain(momentum_params, scalars or None)
     writer = ThreadPoolExecutor(max_workers=1)
     pending = []
     try:
-        dom0 = doms[0]
         cls, _ = dom0.node_class()
         solid = (cls & _abi.LBF_CLASS_SOLID) != 0
         num_fluid = int(np.count_nonzero(~solid))
@@ -160,8 +160,7 @@ def solve(momentum_params: _m.Parameters, passive_scalar_params: Optional[Sequen
         with open(os.path.join(paths["data"], _io.COORDINATES_FILE), "wb") as fh:
             fh.write(("i,j,x,y,node_type\n" if dim == 2 else "i,j,k,x,y,z,node_type\n").encode())
             fh.write(text)
-        for d in doms:
-            d.init(stream)
+        dom0.init(stream)
 
         post_functions = list(momentum_params.post_functions or [])
         res_path = os.path.join(paths["data"], _io.RESIDUALS_FILE)
@@ -174,8 +173,8 @@ def solve(momentum_params: _m.Parameters, passive_scalar_params: Optional[Sequen
                 rho, u, _ = dom0.moments(stream)
                 fields = [("density", "density", rho),
                           ("velocity", ",".join(f"velocity_{x}" for x in "xyz"[:dim]), u)]
-                for d, nm in zip(doms, names):
-                    fields.append((nm, nm, d.moments(stream)[2]))
+                for i, nm in enumerate(names):
+                    fields.append((nm, nm, dom0.scalar(i, stream)))
                 step_path = os.path.join(paths["data"], str(t))
                 os.makedirs(step_path, exist_ok=True)
                 for prefix, hdr, values in fields:
@@ -188,15 +187,9 @@ def solve(momentum_params: _m.Parameters, passive_scalar_params: Optional[Sequen
                 view = LatticeView(dom0, t, num_fluid)
                 for pf in due:
                     post_lines.append((pf, pf.function(view)))
-            for d in doms:
-                d.step(1, 1, stream)
+            dom0.step(1, 1, stream)
             # ---- residuals, post-processing, residual file, stop ---------------
-            r0, _ = doms[0].residuals()
-            res = list(r0[: 1 + dim])
-            for d in doms:
-                if d.has_scalar:
-                    res.append(float(d.residuals()[0][1 + dim]))
-            res = np.array(res)
+            res = np.array(dom0.residuals()[0])
             for pf, results in post_lines:
                 path = os.path.join(paths["post"], pf.file_name)
                 with open(path, "a") as fh:
@@ -224,5 +217,4 @@ def solve(momentum_params: _m.Parameters, passive_scalar_params: Optional[Sequen
                            wall_seconds=time.perf_counter() - wall0)
     finally:
         writer.shutdown(wait=True)
-        for d in doms:
-            d.close()
+        dom0.close()

@@ -30,6 +30,12 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_abi.SIGNATURES), set(names) - set(_abi.SIGNATURES)
 
 
+def test_header_constants_mirrored():
+    with open(os.path.join(ROOT, "include", "lbflow.h")) as fh:
+        src = fh.read()
+    assert int(re.search(r"#define LBF_MAX_SCALARS (\d+)", src).group(1)) == _abi.LBF_MAX_SCALARS
+
+
 def test_abi_version_and_layouts():
     lib = _abi.load()
     assert lib.lbf_abi_version() == 1
