@@ -235,8 +235,9 @@ lbf_status lbf_domain_get_node_class(lbf_domain* dom, uint32_t* node_class, uint
  * LBF_OPT_PIPE_STAGES  ring depth of the pipelined sweep (0 = from the smem budget).
  * LBF_OPT_COMPACT  1 = on the lean path, sweep a list of the fluid nodes (plus solid
  *                  nodes sharing a 32-byte sector with them) instead of the dense
- *                  lattice; default on for FP64 storage only (where it is faster); set
- *                  before lbf_domain_init.  get: 1 when in effect.
+ *                  lattice; default on for FP64 storage and for D3Q27 other than MRT
+ *                  (where it is faster); set before lbf_domain_init.  get: 1 when in
+ *                  effect.
  * LBF_OPT_Z_BEGIN, LBF_OPT_Z_END  planes [z_begin, z_end) that steps, observation and
  *                  inventories cover (default all); set before lbf_domain_init.  A
  *                  z-slab of a larger lattice sweeps its owned planes and keeps one

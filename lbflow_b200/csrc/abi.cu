@@ -337,7 +337,7 @@ struct lbf_domain {
     bool pipe = false;            // pipelined bulk-copy sweep on the lean path (option)
     int pipe_stages = 0;          // 0 = chosen from the shared-memory budget
     bool compact = false;         // compacted sweep over a work list on the lean path (in effect)
-    int compact_opt = -1;         // -1 = default (FP64 storage only), 0 off, 1 on
+    int compact_opt = -1;         // -1 = default (FP64 storage, D3Q27), 0 off, 1 on
     long long z_begin = 0, z_end = 0;   // planes swept (0, 0 = all); a z-slab sweeps its owned planes
     int sparse_opt = -1;          // fluid-only layout on the lean path: 1 on, 0 off, -1 auto (>= 5 % solid)
     bool sparse = false;          // the sparse layout is in effect: list = fluid cells, pop planes of Np fluid slots
@@ -779,7 +779,13 @@ lbf_status prepare(lbf_domain* D, uint32_t* cls_out, uint32_t* links_out, cudaSt
             if (!D->gpop[si][k] && (st = dmalloc(D, &D->gpop[si][k], (size_t)D->q * D->Np * rt_bytes(D->st))))
                 return st;
     }
-    const bool want = (D->compact_opt < 0 ? D->st == LBF_STORE_F64 : D->compact_opt != 0) && !z_restricted(D);
+    // the work list wins for FP64 and for D3Q27 (its 256-thread blocks fit 64
+    // registers, four per SM, for BGK, TRT and central moments; the dense D3Q27
+    // sweep keeps 128): Taylor-Green 384^3, central, FP32 24.5k MLUPS against
+    // 16.3k dense, FP16 deviations 25.4k against 18.8k.  D3Q27 MRT (the 27 x 27
+    // population-space matrix) spills at 64 registers and stays dense.
+    const bool dflt = D->st == LBF_STORE_F64 || (D->vs == LBF_D3Q27 && D->desc.collision.kind != LBF_MRT);
+    const bool want = (D->compact_opt < 0 ? dflt : D->compact_opt != 0) && !z_restricted(D);
     D->compact = want;
     if (!D->facebc && !D->scalar && want && N < (1ll << 30) && (st = build_list(D, s))) return st;
     D->prepared = true;
@@ -1990,7 +1996,7 @@ void batch_harvest(lbf_batch* b) {
             const BatchState& s = g.host[p];
             D->t = s.done_t >= 0 ? s.done_t + 1 : s.t0;
             if (s.res_t >= 0) {
-                for (int i = 0; i < 5; ++i) D->res_host[i] = s.res[i];
+                for (int i = 0; i < 8; ++i) D->res_host[i] = s.res[i];
                 D->res_step = s.res_t;
             }
             D->last_stream = b->last;
@@ -2054,6 +2060,13 @@ cudaError_t batch_launch_finalize(const lbf_batch::Group& g, cudaStream_t s) {
 }
 
 // New groups, device tables and chunk graph for the current members.
+// Domains that the batched kernels do not cover (scalars, the central-moment
+// collision, the sparse layout with explicit faces) run their own single-domain
+// sweep inside the chunk graph, gated by their batch state like the large members.
+bool solo_only(const lbf_domain* D) {
+    return D->scalar || D->desc.collision.kind == LBF_CENTRAL || (D->sparse && D->facebc);
+}
+
 lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
     if (b->launched) CK(cudaEventSynchronize(b->ev));
     if (b->launched) batch_harvest(b);
@@ -2078,7 +2091,7 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         // a large member runs its own sweep in the graph; its launch parameters are
         // fixed per chunk step only when k is even (t0 keeps its parity)
         const long long units = D->sparse ? D->nlist : D->N;
-        const bool solo = b->k % 2 == 0 && (units >= SOLO_UNITS || (D->sparse && D->facebc)) && !D->pipe && !D->stage;
+        const bool solo = b->k % 2 == 0 && (units >= SOLO_UNITS || solo_only(D)) && !D->pipe && !D->stage;
         lbf_batch::Group* g = nullptr;
         for (auto& x : b->groups)
             if (!solo && !x.solo && x.vs == D->vs && x.coll == coll && x.st == D->st && x.facebc == D->facebc &&
@@ -2121,10 +2134,10 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
             x.block0 = (long long)blk.size();
             x.done_t = -1;
             x.res_t = D->res_step;
-            for (int i = 0; i < 5; ++i) x.res[i] = D->res_host[i];
+            for (int i = 0; i < 8; ++i) x.res[i] = D->res_host[i];
             x.k = b->k;
             x.d = D->d;
-            x.has_scalar = D->scalar ? 1 : 0;
+            x.ns = D->ns;
             for (int i = 0; i < 3; ++i) x.tol[i] = m.tol[i];
             blk.insert(blk.end(), (size_t)nb, (int)p);
         }
@@ -2263,12 +2276,13 @@ lbf_status lbf_batch_admit(lbf_batch* b, lbf_domain* D, int64_t max_iterations, 
     std::lock_guard<std::mutex> lock(b->mu);
     if (D->batch) return fail(LBF_ESTATE, "the domain is already in a batch");
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before lbf_batch_admit");
-    if (D->scalar) return fail(LBF_EUNSUPPORTED, "domains with a scalar are not batched");
-    if (D->desc.collision.kind == LBF_CENTRAL)
-        return fail(LBF_EUNSUPPORTED, "domains with the central-moment collision are not batched");
-    if (D->sparse && D->facebc && b->k % 2)
-        return fail(LBF_EUNSUPPORTED, "a sparse-layout domain with explicit faces is batched with an even residual "
-                                      "interval only (it runs its own sweep in the chunk graph)");
+    if (solo_only(D) && b->k % 2)
+        return fail(LBF_EUNSUPPORTED, "a domain with scalars, the central-moment collision or the sparse layout with "
+                                      "explicit faces is batched with an even residual interval only (it runs its own "
+                                      "sweep in the chunk graph)");
+    if (solo_only(D) && (D->pipe || D->stage))
+        return fail(LBF_EUNSUPPORTED, "a domain that runs its own sweep in a batch takes neither the pipelined nor "
+                                      "the staged sweep");
     if (z_restricted(D)) return fail(LBF_EUNSUPPORTED, "z-slab domains are not batched");
     if (max_iterations < 0) return fail(LBF_EINVAL, "max_iterations must be >= 0");
     lbf_status st;

@@ -19,10 +19,10 @@ struct BatchState {
     long long res_t;    // time step of res[] (-1 = none yet)
     int k;              // residual interval (chunk length)
     int status;         // 0 running, 1 converged, 2 max_iterations, 3 non-finite residual
-    int has_scalar;
+    int ns;             // scalars (their residuals are accumulators 4 .. 4 + ns - 1)
     int d;
     double tol[3];      // density, velocity, scalar tolerances
-    double res[8];      // residuals of res_t: rho, u_0.., (C at 4), as k_finalize writes them
+    double res[8];      // residuals of res_t: rho, u_0.., scalars from 4, as k_finalize writes them
 };
 
 // Launches one time step (chunk step j) of every domain in a batch group: all

@@ -167,7 +167,8 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
     __shared__ double r[8];
     __shared__ double part[256];
     // the per-block partials of the residual step, summed in slot order
-    for (int a = 0; a < 5; ++a) {
+    const int nacc = s.ns > 0 ? 4 + s.ns : 5;
+    for (int a = 0; a < nacc; ++a) {
         double sum = 0.0;
         for (long long jj = threadIdx.x; jj < nslots; jj += blockDim.x) sum += accum[a * stride + jj];
         part[threadIdx.x] = sum;
@@ -181,14 +182,14 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
     }
     if (threadIdx.x == 0) {
         if (ran) {
-            for (int i = 0; i < 5; ++i) s.res[i] = r[i];
+            for (int i = 0; i < nacc; ++i) s.res[i] = r[i];
             s.res_t = t_end;
         }
         const bool max_stop = t_end >= s.last_t;   // a step t > max_iterations ran
         if (ran && !max_stop && t_end > 10) {
             bool conv = r[0] <= s.tol[0];
             for (int i = 0; i < s.d; ++i) conv = conv && r[1 + i] <= s.tol[1];
-            if (s.has_scalar) conv = conv && r[4] <= s.tol[2];
+            for (int i = 0; i < s.ns; ++i) conv = conv && r[4 + i] <= s.tol[2];
             if (!isfinite(r[0])) {
                 s.status = 3;
                 s.done_t = t_end;

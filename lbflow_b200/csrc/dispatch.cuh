@@ -135,6 +135,12 @@ cudaError_t launch_step_sparse_fs(int st, bool scalar, const StepParams& base, c
                                   cudaStream_t stream);
 #define LBF_SPARSE_FS_CASE(V_, C_, S_, SC_)                                                    \
     if (st == S_ && scalar == SC_) {                                                           \
+        /* bulk launches prefetch one wave ahead (the blocks the launch bounds keep    */      \
+        /* resident on every SM); the face pass has no wave to look ahead to          */      \
+        int dev_ = 0, sms_ = 0;                                                                \
+        cudaGetDevice(&dev_);                                                                  \
+        cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_);                   \
+        kp.pf_blocks = kp.face_pass ? 0 : sms_ * sparse_fs_blocks<V_, C_, S_, SC_>();           \
         k_step_sparse_fs<V_, C_, S_, true, SC_><<<blocks, 256, 0, stream>>>(kp);                \
         return cudaGetLastError();                                                             \
     }

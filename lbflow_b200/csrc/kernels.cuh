@@ -2050,8 +2050,13 @@ __device__ __forceinline__ void sparse_prefetch(const KParams<VS>& P) {
     if (!P.first) {
         sfor<L::Q>([&](auto I) {
             constexpr int i = I;
-            if constexpr (L::c(i, 1) == 0 && (L::D == 2 || L::c(i, 2) == 0))
+            if constexpr (L::c(i, 1) == 0 && (L::D == 2 || L::c(i, 2) == 0)) {
                 pf((const T*)P.srcp[i] + k0, n * (long long)sizeof(T));
+                // the scalars' planes of the same directions (compute type)
+                for (int si = 0; si < P.nscalar; ++si)
+                    pf((const typename Store<ST>::R*)P.sc[si].gsrc + (long long)i * P.np + k0,
+                       n * (long long)sizeof(typename Store<ST>::R));
+            }
         });
     }
 }
@@ -2175,6 +2180,7 @@ __global__ void __launch_bounds__(256, (sparse_fs_blocks<VS, COLL, ST, SCALAR>()
     Geo g;
     uint32_t mk;
     int k;
+    if (!(FACEBC && P.face_pass)) sparse_prefetch<VS, ST>(P);
     const bool valid = sparse_fs_node<FACEBC>(P, tid, g, k, mk);
     double racc[5] = {};
     if (valid) {

@@ -225,3 +225,81 @@ def test_batch_large_members_run_their_own_sweep(env):
         gs, gr, gu = got[i]
         assert gs == steps, (i, gs, steps)
         assert rel(gr[fl], rho[fl]) <= tol and rel(gu[fl], u[fl]) <= tol, i
+
+
+def _scalar_mix():
+    """Members the batched kernels do not cover, which run their own sweep in the
+    chunk graph: a D2Q9 channel with a scalar (dense layout), a packed bed with
+    two scalars (sparse layout, outflow face pass), a D3Q27 central-moment vortex;
+    plus a small lean cavity in a batched launch beside them."""
+    from lbflow_b200 import passive_scalar as ps
+    from lbflow_b200.core import TRT
+    ch = _channel_d2q9()
+    s_ch = ps.Parameters(scalar_name="c", collision_operator=BGK(0.6), velocity_set=VelocitySet.D2Q9,
+                         initial_scalar_value=ps.InitialScalarValue.Uniform(0.0),
+                         boundary_conditions=[(W, ps.AntiBounceBack(1.0)), (E, ps.AntiBBNoFlux),
+                                              (S, ps.BBNoFlux), (N, ps.BBNoFlux)],
+                         inner_boundary_condition=ps.InnerBounceBack)
+    n = [14, 12, 24]
+    bed, s0 = cases.packed_bed_scalar(n, mask=cases.sphere_pack(n, 0.7, 1.5, 2.5, seed=4), storage=Storage.F32,
+                                      ka=1e-2)
+    s1 = ps.Parameters(scalar_name="tracer", collision_operator=TRT.from_magic(0.7), velocity_set=VelocitySet.D3Q19,
+                       initial_scalar_value=ps.InitialScalarValue.Uniform(0.1),
+                       boundary_conditions=[(W, ps.BBNoFlux), (E, ps.BBNoFlux), (S, ps.BBNoFlux), (N, ps.BBNoFlux),
+                                            (BoundaryFace.Bottom, ps.AntiBounceBack(0.5)),
+                                            (BoundaryFace.Top, ps.SecondOrderNoFlux(unknown_populations_only=False))],
+                       inner_boundary_condition=ps.InnerBounceBack)
+    return [(ch, [s_ch], 1e-12), (bed, [s0, s1], 1e-5),
+            (cases.tgv_d3q27(12, 0.05, 20.0, Storage.F64, collision="central")[0], None, 1e-12),
+            (cases.cavity_d2q9(20, 0.6, 0.1, Storage.F32), None, 1e-5)]
+
+
+def test_batch_scalar_and_central_domains_match_alone(env):
+    Domain, Batch, _ = env
+    mix = _scalar_mix()
+    max_it = 200
+    alone = []
+    for p, sps, _ in mix:
+        with Domain(p, sps) as d:
+            d.init()
+            steps = d.run(max_it, K, 1e-7, 1e-7, 1e-7)
+            rho, u, _ = d.moments()
+            cs = [d.scalar(i) for i in range(d.num_scalars)]
+            res, _ = d.residuals()
+            cls, _ = d.node_class()
+        alone.append((steps, rho, u, cs, res, (cls & _abi.LBF_CLASS_SOLID) == 0))
+    with Batch(0, K) as batch:
+        live = {}
+        for i, (p, sps, _) in enumerate(mix):
+            d = Domain(p, sps).init()
+            batch.admit(d, max_it, 1e-7, 1e-7, 1e-7)
+            live[d.h.value] = (i, d)
+        got = {}
+        for _ in range(200):
+            if not live:
+                break
+            batch.step(2)
+            for dom, status in batch.poll(wait=True):
+                i, d = live.pop(dom.h.value)
+                rho, u, _ = d.moments()
+                got[i] = (d.time_step, rho, u, [d.scalar(j) for j in range(d.num_scalars)], d.residuals()[0])
+                d.close()
+    assert not live
+    for i, (p, sps, tol) in enumerate(mix):
+        steps, rho, u, cs, res, fl = alone[i]
+        gs, gr, gu, gc, gres = got[i]
+        assert gs == steps, (i, gs, steps)
+        assert rel(gr[fl], rho[fl]) <= tol and rel(gu[fl], u[fl]) <= tol, i
+        assert len(gc) == len(cs) and len(gres) == len(res)
+        for a, b in zip(gc, cs):
+            assert rel(a[fl], b[fl]) <= tol, i
+        assert np.allclose(gres, res, rtol=1e-9, atol=0), i
+
+
+def test_batch_scalar_domain_needs_even_interval(env):
+    Domain, Batch, _ = env
+    p, sps, _ = _scalar_mix()[0]
+    with Batch(0, 5) as batch, Domain(p, sps) as d:
+        d.init()
+        with pytest.raises(RuntimeError, match="EUNSUPPORTED"):
+            batch.admit(d, 100)
