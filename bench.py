@@ -304,17 +304,25 @@ def measure_e2e(args, p, n_fluid, N, stream, world):
     import torch
     import torch.distributed as dist
     from lbflow_b200.domain import Domain, solve_arrays
+    # the results land in page-locked host buffers, allocated before the timed
+    # region (a serving caller keeps them): the library copies into them directly
+    d = p.dim
+    out = tuple(torch.empty(n, dtype=torch.float64, pin_memory=True).numpy() for n in (N, N * d))
+    out = (out[0], out[1], None)
+    solve_arrays(p, args.steps, stream=stream, out=out)   # warm-up solve (pool, pinned staging, module loads)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
+    reps = 3
     t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     wall0 = time.perf_counter()
-    solve_arrays(p, args.steps, stream=stream)
+    for _ in range(reps):
+        solve_arrays(p, args.steps, stream=stream, out=out)
     t1.record(stream)
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
-    e_sec = max(t0.elapsed_time(t1) / 1e3, wall)
+    e_sec = max(t0.elapsed_time(t1) / 1e3, wall) / reps
     if world > 1:
         t = torch.tensor([e_sec], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -329,7 +337,7 @@ def measure_e2e(args, p, n_fluid, N, stream, world):
     sync(); c2 = time.perf_counter()
     dom.step(args.steps, 0, stream)
     sync(); c3 = time.perf_counter()
-    dom.moments(stream)
+    dom.moments(stream, out=out)
     sync(); c4 = time.perf_counter()
     dom.close()
     sync(); c5 = time.perf_counter()
@@ -339,9 +347,10 @@ def measure_e2e(args, p, n_fluid, N, stream, world):
             "h2d_bytes_per_step": N / args.steps, "d2h_bytes_per_step": N * (1 + 3) * 8 / args.steps,
             "ms_per_solve": 1e3 * e_sec,
             "split": split,
-            "note": f"lbf_solve per solve of {args.steps} steps: node-type upload (N x 1 B), layout build, init, "
-                    f"{args.steps} steps, FP64 density + velocity download (N x 32 B); split measured on a second "
-                    "solve through the separate calls"}
+            "note": f"lbf_solve per solve of {args.steps} steps (mean of {reps} after one warm-up solve): "
+                    f"node-type upload (N x 1 B), layout build, init, {args.steps} steps, FP64 density + velocity "
+                    "download (N x 32 B) into page-locked host buffers; split measured on a further solve through "
+                    "the separate calls"}
 
 
 def accuracy_vs_oracle(args, mask, steps, storages, threads=0):

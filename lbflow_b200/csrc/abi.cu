@@ -11,9 +11,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
@@ -173,7 +175,12 @@ void host_copy_parallel(char* dst, const char* src, size_t bytes) {
 }
 
 cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t s) {
-    if (bytes < (4u << 20)) {
+    // page-locked caller memory (cudaMallocHost, cudaHostRegister, a pinned tensor):
+    // one direct copy at the full link rate
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, dst) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    if (!pinned) cudaGetLastError();   // pageable memory is not an error
+    if (pinned || bytes < (4u << 20)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
         return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
     }
@@ -290,6 +297,21 @@ void tables_of(int* d, int* q, int* c, double* w, int* qbar, int* qfaces, int* n
 
 // ============================================================== the domain
 struct lbf_batch;
+// An allocator whose resize leaves the new elements uninitialised (the caller
+// writes every one): a lattice-sized host array is then touched once, not twice.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept { ::new ((void*)p) U; }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+};
+
 struct lbf_domain {
     lbf_domain_desc desc{};
     int vs = 0, q = 0, d = 0, st = 0, nfaces = 0;
@@ -299,7 +321,7 @@ struct lbf_domain {
     bool facebc = false, prepared = false, initialized = false;
     unsigned folded = 0;   // no-slip faces applied through the link bits of the pull
     // host copies of the inputs (solid-node outputs, re-initialisation)
-    std::vector<uint8_t> type;
+    std::vector<uint8_t, NoInitAlloc<uint8_t>> type;   // filled once, in lbf_domain_create
     std::vector<double> rho0, u0;
     double rho0u = 1.0, u0u[3] = {0, 0, 0};
     // passive scalars (passive_scalar::LatticeVec): one momentum sweep advances all
@@ -1344,11 +1366,14 @@ lbf_status lbf_domain_create(const lbf_domain_desc* ds, lbf_domain** out) {
     D->vs = vs; D->q = vs_q(vs); D->d = d; D->st = ds->storage; D->nfaces = nf;
     for (int a = 0; a < 3; ++a) D->n[a] = n[a];
     D->N = N;
-    D->type.assign(N, 0);
+    D->type.resize((size_t)N);
     if (ds->node_type) {
-        std::memcpy(D->type.data(), ds->node_type, (size_t)N);
-        // any non-zero value means solid: normalised to 1 (a no-op for 0 / 1 masks)
-        for (long long i = 0; i < N; ++i) D->type[i] = D->type[i] != 0;
+        // any non-zero value means solid: normalised to 1, in one pass
+        const uint8_t* src = ds->node_type;
+        uint8_t* dst = D->type.data();
+        for (long long i = 0; i < N; ++i) dst[i] = src[i] != 0;
+    } else {
+        std::memset(D->type.data(), 0, (size_t)N);
     }
     D->rho0u = ds->initial_density;
     for (int a = 0; a < 3; ++a) D->u0u[a] = ds->initial_velocity[a];

@@ -145,13 +145,13 @@ class Domain:
         _abi.check(self.lib.lbf_domain_residuals(self.h, _ptr(out), C.byref(t)))
         return out[: 1 + self.d + self.num_scalars], t.value
 
-    def moments(self, stream=None):
-        """(density[N], velocity[N, D], scalar[N] or None) at the current time step."""
-        rho = np.zeros(self.N)
-        u = np.zeros(self.N * self.d)
-        c = np.zeros(self.N) if self.has_scalar else None
+    def moments(self, stream=None, out=None):
+        """(density[N], velocity[N, D], scalar[N] or None) at the current time step.
+        `out` = (rho, u, c) preallocated float64 arrays (any may be None) to fill;
+        page-locked ones (e.g. numpy views of pinned tensors) download directly."""
+        rho, u, c = _outputs(self.N, self.d, self.has_scalar, out)
         _abi.check(self.lib.lbf_domain_get_moments(self.h, _ptr(rho), _ptr(u), _ptr(c), _stream_handle(stream)))
-        return rho, u.reshape(self.N, self.d), c
+        return rho, (u.reshape(self.N, self.d) if u is not None else None), c
 
     def scalar(self, index: int = 0, stream=None) -> np.ndarray:
         """Scalar `index` (attach order) at the current time step, [N]."""
@@ -206,8 +206,21 @@ def tables(vs: int) -> dict:
             "mrt_inverse": Mi[:q * q].reshape(q, q)}
 
 
-def solve_arrays(params: _m.Parameters, nsteps: int, scalar: Optional[_ps.Parameters] = None, stream=None):
-    """lbf_solve: one call with host buffers (create, init, nsteps main_steps, moments)."""
+def _outputs(N: int, d: int, has_scalar: bool, out):
+    """Output arrays (rho[N], u[N*D], c[N] or None): the caller's, checked, or new."""
+    if out is None:
+        return np.zeros(N), np.zeros(N * d), (np.zeros(N) if has_scalar else None)
+    rho, u, c = out
+    for a, n in ((rho, N), (u, N * d), (c, N)):
+        if a is not None and (a.dtype != np.float64 or a.size != n or not a.flags.c_contiguous):
+            raise ValueError(f"output arrays must be contiguous float64 of {n} elements")
+    return rho, (u.reshape(-1) if u is not None else None), (c if has_scalar else None)
+
+
+def solve_arrays(params: _m.Parameters, nsteps: int, scalar: Optional[_ps.Parameters] = None, stream=None,
+                 out=None):
+    """lbf_solve: one call with host buffers (create, init, nsteps main_steps, moments).
+    `out` = (rho, u, c) preallocated float64 arrays to fill, as in Domain.moments."""
     lib = _abi.load()
     desc, keep = _m.to_desc(params)
     vs = VelocitySet(desc.velocity_set)
@@ -216,7 +229,7 @@ def solve_arrays(params: _m.Parameters, nsteps: int, scalar: Optional[_ps.Parame
     if scalar is not None:
         sdesc, k2 = _ps.to_desc(scalar, [desc.n[a] for a in range(vs.d)])
         keep += k2
-    rho = np.zeros(N); u = np.zeros(N * vs.d); c = np.zeros(N) if scalar is not None else None
+    rho, u, c = _outputs(N, vs.d, scalar is not None, out)
     _abi.check(lib.lbf_solve(C.byref(desc), C.byref(sdesc) if sdesc is not None else None, int(nsteps),
                              _ptr(rho), _ptr(u), _ptr(c), _stream_handle(stream)))
-    return rho, u.reshape(N, vs.d), c
+    return rho, (u.reshape(N, vs.d) if u is not None else None), c
