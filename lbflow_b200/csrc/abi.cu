@@ -379,11 +379,17 @@ struct lbf_domain {
     long long Np = 0;             // population plane stride: N rounded up to 64 nodes
     int* err = nullptr;           // device flag: a bounded wait gave up
     cudaStream_t last_stream = nullptr;
+    // the side stream and events of the face-pass overlap (do_steps), made on first use
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_bulk = nullptr, ev_head = nullptr;
     long long bytes = 0;
     lbf_batch* batch = nullptr;   // set while the domain is admitted to a batch
     int dev = 0;                  // device that holds the domain's memory
 
     ~lbf_domain() {
+        if (ev_bulk) cudaEventDestroy(ev_bulk);
+        if (ev_head) cudaEventDestroy(ev_head);
+        if (side) cudaStreamDestroy(side);
         for (int k = 0; k < 2; ++k) {
             dev_free(pop[k], dev); dev_free(mom[k], dev);
             for (int f = 0; f < 6; ++f) dev_free(pb[f][k], dev);
@@ -976,13 +982,41 @@ cudaError_t launch_list(lbf_domain* D, const StepParams& P, cudaStream_t s) {
 
 // Sparse sweep with explicit faces and/or the scalar: the bulk launch, then one
 // face pass per scalar outflow face (as launch_step_any does for the dense sweep).
+cudaError_t sparse_fs_launch(lbf_domain* D, const StepParams& Q, unsigned blocks, cudaStream_t s) {
+    return by_kind(D, [&](auto V, auto C) {
+        return launch_step_sparse_fs<decltype(V)::value, decltype(C)::value>(D->st, D->scalar, Q, lam_of(D), blocks,
+                                                                             s);
+    });
+}
+
+// The bulk launch of the sparse face/scalar sweep over the fluid slots [kb, ke).
+cudaError_t sparse_fs_bulk(lbf_domain* D, const StepParams& P, long long kb, long long ke, cudaStream_t s) {
+    if (ke <= kb) return cudaSuccess;
+    StepParams B = P;
+    B.kbeg = kb;
+    B.kend = ke;
+    const unsigned nb = (unsigned)((ke - kb + 255) / 256);
+    take_slots(D, B, nb);
+    return sparse_fs_launch(D, B, nb, s);
+}
+
+// The face passes of the scalar outflow faces (after the bulk launch of the step).
+cudaError_t sparse_fs_faces(lbf_domain* D, const StepParams& P, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    for (int f = 0; f < D->nfaces && e == cudaSuccess; ++f) {
+        if (!(D->outflow >> f & 1u)) continue;
+        StepParams F = P;
+        F.face_pass = 1;
+        F.fp_face = f;
+        const unsigned nf = (unsigned)((D->pb_plane[f] + 255) / 256);
+        take_slots(D, F, nf);
+        e = sparse_fs_launch(D, F, nf, s);
+    }
+    return e;
+}
+
 cudaError_t launch_sparse_fs(lbf_domain* D, const StepParams& P, cudaStream_t s) {
-    auto one = [&](const StepParams& Q, unsigned blocks) -> cudaError_t {
-        return by_kind(D, [&](auto V, auto C) {
-            return launch_step_sparse_fs<decltype(V)::value, decltype(C)::value>(D->st, D->scalar, Q, lam_of(D),
-                                                                                 blocks, s);
-        });
-    };
+    auto one = [&](const StepParams& Q, unsigned blocks) -> cudaError_t { return sparse_fs_launch(D, Q, blocks, s); };
     StepParams B = P;
     const unsigned nb = (unsigned)((P.kend - P.kbeg + 255) / 256);
     take_slots(D, B, nb);
@@ -1133,11 +1167,52 @@ lbf_status do_init(lbf_domain* D, cudaStream_t s) {
     return LBF_OK;
 }
 
+// The outflow face pass of step t runs beside the sweep of step t + 1 over the
+// planes below ZCUT = nz - 4 (on a side stream), when the only outflow face is
+// the top face of a whole lattice in the sparse layout and the bottom and top
+// faces are explicit for the momentum and every scalar.  With buffers X (read
+// by step t) and Y (written):
+//  - the face pass reads X at the top plane and the plane below it, the
+//    snapshots of planes nz - 2 and nz - 3 and the top face's layers, and writes
+//    Y at the top plane and those layers;
+//  - the lower sweep of step t + 1 reads Y at planes <= nz - 4 (all written by
+//    step t's bulk launch, which precedes it) and writes X at planes < nz - 4;
+//  - the pulls that wrap in z (the top plane from plane 0, plane 0 from the top
+//    plane) fetch populations that the explicit bottom and top face rules replace
+//    before any use, so when those reads land relative to the other stream's
+//    writes changes no result.
+// The rest of step t + 1 (planes >= nz - 4) follows the face pass on the main
+// stream, and step t + 2's lower sweep waits for both parts of step t + 1.
+// Steps that compute residuals or write moments, and the first step, run in order.
+constexpr long long OVL_CUT = 4;
+
+bool face_overlap_ok(const lbf_domain* D) {
+    if (!D->sparse || !(D->facebc || D->scalar) || z_restricted(D) || D->d != 3) return false;
+    if (D->outflow != (1u << 5) || D->n[2] < 3 * OVL_CUT) return false;
+    for (int f = 4; f < 6; ++f) {
+        if (D->desc.bc[f].kind == LBF_BC_PERIODIC) return false;
+        for (int si = 0; si < D->ns; ++si)
+            if (D->sdesc[si].bc[f].kind == LBF_SBC_PERIODIC) return false;
+    }
+    return true;
+}
+
 lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s) {
     if (!D->initialized) return fail(LBF_ESTATE, "lbf_domain_init must be called before stepping");
     if (D->part_pending) return fail(LBF_ESTATE, "a split step waits for its part 1");
     lbf_status st;
     if (k > 0 && (st = ensure_mom(D))) return st;
+    const bool ovl = face_overlap_ok(D) && nsteps > 1;
+    if (ovl && !D->side) {
+        CK(cudaStreamCreateWithFlags(&D->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&D->ev_bulk, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&D->ev_head, cudaEventDisableTiming));
+    }
+    const long long kcut = ovl ? D->zoff[(size_t)(D->n[2] - OVL_CUT)] : 0;
+    auto plain = [&](long long t) {   // a step that takes part in no overlap
+        return t == 0 || (k > 0 && (t % k == 0 || (t + 1) % k == 0));
+    };
+    bool head_ran = false;   // the lower sweep of this step already ran on the side stream
     for (long long it = 0; it < nsteps; ++it) {
         const long long t = D->t;
         StepParams P;
@@ -1145,7 +1220,26 @@ lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s
         P.residual = (k > 0 && t % k == 0) ? 1 : 0;
         P.write_mom = (k > 0 && (t % k == 0 || (t + 1) % k == 0)) ? 1 : 0;
         D->slot_next = 0;
-        cudaError_t e = launch_step_any(D, P, s);
+        cudaError_t e;
+        if (ovl) {
+            const bool next = it + 1 < nsteps && !plain(t) && !plain(t + 1);
+            e = sparse_fs_bulk(D, P, head_ran ? kcut : P.kbeg, P.kend, s);
+            if (head_ran && e == cudaSuccess) e = cudaStreamWaitEvent(s, D->ev_head, 0);
+            if (next && e == cudaSuccess) e = cudaEventRecord(D->ev_bulk, s);
+            // the face pass is submitted first, so that its single wave of blocks is
+            // dispatched before the lower sweep's blocks take every SM
+            if (e == cudaSuccess) e = sparse_fs_faces(D, P, s);
+            if (next && e == cudaSuccess) {
+                StepParams N1;
+                base_params(D, N1, t + 1);
+                e = cudaStreamWaitEvent(D->side, D->ev_bulk, 0);
+                if (e == cudaSuccess) e = sparse_fs_bulk(D, N1, N1.kbeg, kcut, D->side);
+                if (e == cudaSuccess) e = cudaEventRecord(D->ev_head, D->side);
+            }
+            head_ran = next;
+        } else {
+            e = launch_step_any(D, P, s);
+        }
         if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
         if (P.residual) {
             k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, D->nacc(), 1, D->res_dev);
