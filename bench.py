@@ -915,7 +915,7 @@ def run_batch_probe(args, rank, world, local_rank):
     ones, and the host cost of one request's lifecycle (create, init, moments, destroy)."""
     import math
     import torch
-    from lbflow_b200 import cases, serve
+    from lbflow_b200 import _abi, cases, serve
     from lbflow_b200.batch import Batch
     from lbflow_b200.core import Storage
     from lbflow_b200.domain import Domain
@@ -959,14 +959,18 @@ def run_batch_probe(args, rank, world, local_rank):
     with Batch(0, 50) as b:
         for d in doms:
             b.admit(d, 10**6, math.inf, 0.0, math.inf)
-        b.step(1)
-        b.poll(wait=True)
-        sync()
-        t = time.perf_counter()
-        b.step(2)
-        b.poll(wait=True)
-        sync()
-        out["small_64x64sq_batched_domain_steps_per_s"] = 64 * 100 / (time.perf_counter() - t)
+        # one launch per step (the default), then a group's chunk in one cooperative launch
+        for chunk, key in ((0, "small_64x64sq_batched_domain_steps_per_s"),
+                           (1, "small_64x64sq_batched_chunk_launch_domain_steps_per_s")):
+            b.set_option(_abi.LBF_BATCH_OPT_CHUNK_LAUNCH, chunk)
+            b.step(1)
+            b.poll(wait=True)
+            sync()
+            t = time.perf_counter()
+            b.step(2)
+            b.poll(wait=True)
+            sync()
+            out[key] = 64 * 100 / (time.perf_counter() - t)
         for d in doms:
             b.evict(d)
     for d in doms:

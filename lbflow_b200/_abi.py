@@ -28,6 +28,7 @@ LBF_COMPAT_REFERENCE, LBF_COMPAT_PHYSICS = range(2)
  LBF_OPT_SPARSE, LBF_OPT_STREAMING, LBF_OPT_SROUND, LBF_OPT_WAIT_LIMIT, LBF_OPT_SEED_OFFSET) = range(12)
 LBF_STREAM_PULL, LBF_STREAM_PUSH, LBF_STREAM_INPLACE = range(3)
 LBF_MAX_SCALARS = 4
+LBF_BATCH_OPT_CHUNK_LAUNCH = 0
 
 LBF_CLASS_SOLID = 0x1
 LBF_CLASS_BOUNCE_BACK = 0x2
@@ -125,6 +126,7 @@ SIGNATURES = {
     "lbf_batch_poll": (_I32, [_P, C.POINTER(_P), _PI32, _I32, _PI32, _I32]),
     "lbf_batch_evict": (_I32, [_P, _P]),
     "lbf_batch_info": (_I32, [_P, _PI64, _PI64, _PI64, _PI64]),
+    "lbf_batch_set_option": (_I32, [_P, _I32, _I64]),
     "lbf_batch_destroy": (_I32, [_P]),
     "lbf_format_csv": (_I32, [_P, _I64, _I32, _P, _I64, _PI64, _I32]),
     "lbf_format_coordinates": (_I32, [_PI64, _I32, _D, _P, _P, _I64, _PI64, _I32]),

@@ -76,6 +76,12 @@ class Batch:
         _abi.check(st)
         self._doms[dom.h.value] = dom
 
+    def set_option(self, option: int, value: int) -> "Batch":
+        """lbf_batch_set_option, e.g. LBF_BATCH_OPT_CHUNK_LAUNCH (1: a group's chunk
+        in one cooperative launch; 0: one launch per step, the default)."""
+        _abi.check(self.lib.lbf_batch_set_option(self.h, int(option), int(value)))
+        return self
+
     def step(self, nchunks: int = 1, stream=None) -> "Batch":
         """Enqueue `nchunks` chunks of residual_interval steps (asynchronous)."""
         _abi.check(self.lib.lbf_batch_step(self.h, int(nchunks), _stream_handle(stream)))

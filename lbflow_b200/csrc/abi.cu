@@ -2027,6 +2027,7 @@ struct lbf_batch {
     };
     std::mutex mu;
     int k = 1;
+    bool chunk_launch = false;         // a group's k steps in one cooperative launch (LBF_BATCH_OPT_CHUNK_LAUNCH)
     long long budget = 0, bytes = 0;
     std::vector<Member> members;
     std::vector<std::pair<lbf_domain*, int>> finished;   // (domain, status) not yet polled
@@ -2169,6 +2170,16 @@ cudaError_t batch_launch_step(const lbf_batch::Group& g, int j, cudaStream_t s) 
             return launch_step_batch<VS_D3Q27>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, j, g.nblocks, s);
     }
 }
+cudaError_t batch_launch_chunk(const lbf_batch::Group& g, int k, cudaStream_t s) {
+    switch (g.vs) {
+        case LBF_D2Q9:
+            return launch_batch_chunk<VS_D2Q9>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, k, g.nblocks, s);
+        case LBF_D3Q19:
+            return launch_batch_chunk<VS_D3Q19>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, k, g.nblocks, s);
+        default:
+            return launch_batch_chunk<VS_D3Q27>(g.coll, g.st, g.facebc, g.sparse, g.tab, g.bs, g.blk, k, g.nblocks, s);
+    }
+}
 cudaError_t batch_launch_finalize(const lbf_batch::Group& g, cudaStream_t s) {
     const int n = (int)g.mem.size();
     switch (g.vs) {
@@ -2287,7 +2298,10 @@ lbf_status batch_rebuild(lbf_batch* b, cudaStream_t s) {
         for (size_t gi = 0; gi < b->groups.size() && e == cudaSuccess; ++gi) {
             lbf_batch::Group& g = b->groups[gi];
             cudaStream_t sg = g.solo || ns == 1 ? b->side[0] : b->side[1 + gi % (size_t)(ns - 1)];
-            for (int j = 0; j < b->k && e == cudaSuccess; ++j) {
+            if (!g.solo && b->chunk_launch && b->k > 1) {
+                e = batch_launch_chunk(g, b->k, sg);   // the chunk's k steps in one launch
+            }
+            for (int j = 0; j < b->k && e == cudaSuccess && !(!g.solo && b->chunk_launch && b->k > 1); ++j) {
                 if (!g.solo) {
                     e = batch_launch_step(g, j, sg);
                     continue;
@@ -2489,6 +2503,19 @@ lbf_status lbf_batch_info(lbf_batch* b, int64_t* running, int64_t* finished, int
     if (bytes) *bytes = b->bytes;
     if (budget) *budget = b->budget;
     return LBF_OK;
+}
+
+lbf_status lbf_batch_set_option(lbf_batch* b, int32_t option, int64_t value) {
+    if (!b) return fail(LBF_EINVAL, "null batch");
+    std::lock_guard<std::mutex> lock(b->mu);
+    switch (option) {
+        case LBF_BATCH_OPT_CHUNK_LAUNCH:
+            if (b->chunk_launch != (value != 0)) b->dirty = true;   // the chunk graph is captured again
+            b->chunk_launch = value != 0;
+            return LBF_OK;
+        default:
+            return fail(LBF_EINVAL, "unknown batch option");
+    }
 }
 
 lbf_status lbf_batch_destroy(lbf_batch* b) {

@@ -33,6 +33,11 @@ struct BatchState {
 template <int VS>
 cudaError_t launch_step_batch(int coll, int st, bool facebc, bool sparse, const void* tab, const BatchState* bs,
                               const int* blk, int j, unsigned nblocks, cudaStream_t s);
+// All k steps of a chunk for every domain of a group in one cooperative launch
+// (grid barriers between the steps); the same results as k launch_step_batch calls.
+template <int VS>
+cudaError_t launch_batch_chunk(int coll, int st, bool facebc, bool sparse, const void* tab, const BatchState* bs,
+                               const int* blk, int k, unsigned nblocks, cudaStream_t s);
 // Residuals + stop rule + t0 += k for each of the n domains of a group.
 template <int VS>
 cudaError_t launch_batch_finalize(const void* tab, BatchState* bs, int n, cudaStream_t s);

@@ -15,6 +15,10 @@
 // layout form their own groups, swept by k_step_batch_sparse.
 #pragma once
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "batch.cuh"
 
 namespace lbf {
@@ -54,23 +58,24 @@ __device__ __forceinline__ void batch_params(KParams<VS>& Ps, const KParams<VS>*
     __syncthreads();
 }
 
+// Block vb of the batched dense sweep, chunk step j (Ps: the block's shared copy
+// of its domain's parameters).
 template <int VS, int COLL, int ST, bool FACEBC>
-__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
-    k_step_batch(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs, const int* __restrict__ blk,
-                 int j) {
+__device__ __forceinline__ void batch_dense_block(const KParams<VS>* __restrict__ tab,
+                                                  const BatchState* __restrict__ bs, const int* __restrict__ blk,
+                                                  int vb, int j, KParams<VS>& Ps) {
     using L = Lat<VS>;
     using S = Store<ST>;
     using R = typename S::R;
     using T = typename S::T;
     constexpr int Q = L::Q, D = L::D;
-    __shared__ KParams<VS> Ps;
-    const int e = blk[blockIdx.x];
+    const int e = blk[vb];
     const long long t = bs[e].t0 + j;
     if (bs[e].done_t >= 0 || t > bs[e].last_t) return;   // uniform over the block
     batch_params<VS, COLL>(Ps, tab, e, t, bs[e].k);
     const KParams<VS>& P = Ps;
 
-    const long long c64 = (long long)(blockIdx.x - bs[e].block0) * BATCH_BLOCK + threadIdx.x;
+    const long long c64 = (long long)(vb - bs[e].block0) * BATCH_BLOCK + threadIdx.x;
     const bool inside = c64 < P.N;
     Geo g;
     g.cell = inside ? (int)c64 : 0;
@@ -127,28 +132,90 @@ __global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, fa
         const unsigned grp = (per >= 32 ? 0xffffffffu : ((1u << per) - 1u) << ((lane / per) * per));
         if (inside && (mk & M_SOLID) && (fl & grp)) sfor<Q>([&](auto I) { S::st(P.dstp[I], g.cell, R(0)); });
     }
-    if (P.residual) step_partials<5>(racc, P, blockIdx.x - bs[e].block0);
+    if (P.residual) step_partials<5>(racc, P, vb - bs[e].block0);
+}
+
+template <int VS, int COLL, int ST, bool FACEBC>
+__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
+    k_step_batch(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs, const int* __restrict__ blk,
+                 int j) {
+    __shared__ KParams<VS> Ps;
+    batch_dense_block<VS, COLL, ST, FACEBC>(tab, bs, blk, blockIdx.x, j, Ps);
 }
 
 // The batched sweep over domains in the sparse (fluid-only) layout: block b
 // covers 256 fluid nodes of domain blk[b], in fluid order.
 template <int VS, int COLL, int ST>
-__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
-    k_step_batch_sparse(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs,
-                        const int* __restrict__ blk, int j) {
-    __shared__ KParams<VS> Ps;
-    const int e = blk[blockIdx.x];
+__device__ __forceinline__ void batch_sparse_block(const KParams<VS>* __restrict__ tab,
+                                                   const BatchState* __restrict__ bs, const int* __restrict__ blk,
+                                                   int vb, int j, KParams<VS>& Ps) {
+    const int e = blk[vb];
     const long long t = bs[e].t0 + j;
     if (bs[e].done_t >= 0 || t > bs[e].last_t) return;   // uniform over the block
     batch_params<VS, COLL>(Ps, tab, e, t, bs[e].k);
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    const long long k = (long long)(blockIdx.x - bs[e].block0) * BATCH_BLOCK + threadIdx.x;
+    const long long k = (long long)(vb - bs[e].block0) * BATCH_BLOCK + threadIdx.x;
     // the sweep mode is uniform over the block (one domain per block)
     if (Ps.sweep_mode == SWEEP_AA_EVEN) sparse_node<VS, COLL, ST, SWEEP_AA_EVEN>(Ps, k, racc);
     else if (Ps.sweep_mode == SWEEP_AA_ODD) sparse_node<VS, COLL, ST, SWEEP_AA_ODD>(Ps, k, racc);
     else if (Ps.sweep_mode == SWEEP_PUSH) sparse_node<VS, COLL, ST, SWEEP_PUSH>(Ps, k, racc);
     else sparse_node<VS, COLL, ST, SWEEP_PULL>(Ps, k, racc);
-    if (Ps.residual) step_partials<5>(racc, Ps, blockIdx.x - bs[e].block0);
+    if (Ps.residual) step_partials<5>(racc, Ps, vb - bs[e].block0);
+}
+
+template <int VS, int COLL, int ST>
+__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
+    k_step_batch_sparse(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs,
+                        const int* __restrict__ blk, int j) {
+    __shared__ KParams<VS> Ps;
+    batch_sparse_block<VS, COLL, ST>(tab, bs, blk, blockIdx.x, j, Ps);
+}
+
+// All k steps of a chunk in one cooperative launch over the group's packed block
+// index: block b of the grid takes blocks b, b + gridDim.x, .. of each step, and
+// a grid barrier separates the steps (a domain's step j + 1 reads what all its
+// blocks wrote in step j).  The grid is at most what fits on the GPU at once,
+// which the cooperative launch checks, so every barrier completes.  A domain
+// computes the same values as in the one-launch-per-step form: the same blocks,
+// the same per-node code.
+template <int VS, int COLL, int ST, bool FACEBC, bool SPARSE>
+__global__ void __launch_bounds__(BATCH_BLOCK, 2 * light_kernel<VS, COLL, ST, false>())
+    k_step_batch_chunk(const KParams<VS>* __restrict__ tab, const BatchState* __restrict__ bs,
+                       const int* __restrict__ blk, int nvb, int k) {
+    __shared__ KParams<VS> Ps;
+    cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+    for (int j = 0; j < k; ++j) {
+        for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+            __syncthreads();   // the previous block's parameters are no longer read
+            if constexpr (SPARSE) batch_sparse_block<VS, COLL, ST>(tab, bs, blk, vb, j, Ps);
+            else batch_dense_block<VS, COLL, ST, FACEBC>(tab, bs, blk, vb, j, Ps);
+        }
+        if (j + 1 < k) grid.sync();
+    }
+}
+
+template <int VS, int COLL, int ST, bool FACEBC, bool SPARSE>
+cudaError_t launch_batch_chunk_k(const void* tab, const BatchState* bs, const int* blk, int k, unsigned nvb,
+                                 cudaStream_t s) {
+    auto kern = k_step_batch_chunk<VS, COLL, ST, FACEBC, SPARSE>;
+    int per = 0, dev = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, BATCH_BLOCK, 0);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if (per < 1) return cudaErrorInvalidConfiguration;
+    const unsigned grid = (unsigned)std::min<long long>((long long)nvb, (long long)per * sms);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(BATCH_BLOCK);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, (const KParams<VS>*)tab, bs, blk, (int)nvb, k);
 }
 
 // One block of 256 threads per domain: residuals of the chunk's last step (its
@@ -216,7 +283,14 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
         k_step_batch_sparse<VS, C_, S_><<<nblocks, BATCH_BLOCK, 0, s>>>((const KParams<VS>*)tab, bs, blk, j); \
         return cudaGetLastError();                                                                 \
     }
+#define LBF_BATCH_CHUNK_CASE(C_, S_, FB_, SP_)                                                     \
+    if (coll == C_ && st == S_ && facebc == FB_ && sparse == SP_)                                  \
+        return launch_batch_chunk_k<VS, C_, S_, FB_, SP_>(tab, bs, blk, k, nblocks, s);
 #define LBF_BATCH_ST(C_, S_) LBF_BATCH_CASE(C_, S_, false) LBF_BATCH_CASE(C_, S_, true) LBF_BATCH_SPARSE_CASE(C_, S_)
+#define LBF_BATCH_CHUNK_ST(C_, S_) LBF_BATCH_CHUNK_CASE(C_, S_, false, false) LBF_BATCH_CHUNK_CASE(C_, S_, true, false) \
+    LBF_BATCH_CHUNK_CASE(C_, S_, false, true)
+#define LBF_BATCH_CHUNK_COLL(C_) LBF_BATCH_CHUNK_ST(C_, ST_F64) LBF_BATCH_CHUNK_ST(C_, ST_F32) \
+    LBF_BATCH_CHUNK_ST(C_, ST_F16) LBF_BATCH_CHUNK_ST(C_, ST_BF16)
 #define LBF_BATCH_COLL(C_) LBF_BATCH_ST(C_, ST_F64) LBF_BATCH_ST(C_, ST_F32) LBF_BATCH_ST(C_, ST_F16) LBF_BATCH_ST(C_, ST_BF16)
 
 #define LBF_INSTANTIATE_BATCH(VS_)                                                                 \
@@ -227,6 +301,15 @@ __global__ void k_batch_finalize(const KParams<VS>* __restrict__ tab, BatchState
         constexpr int VS = VS_;                                                                    \
         if (nblocks == 0) return cudaSuccess;                                                      \
         LBF_BATCH_COLL(COLL_BGK) LBF_BATCH_COLL(COLL_TRT) LBF_BATCH_COLL(COLL_MRT)                 \
+        return cudaErrorInvalidValue;                                                              \
+    }                                                                                              \
+    template <>                                                                                    \
+    cudaError_t launch_batch_chunk<VS_>(int coll, int st, bool facebc, bool sparse, const void* tab,    \
+                                        const BatchState* bs, const int* blk, int k, unsigned nblocks,  \
+                                        cudaStream_t s) {                                           \
+        constexpr int VS = VS_;                                                                    \
+        if (nblocks == 0 || k == 0) return cudaSuccess;                                            \
+        LBF_BATCH_CHUNK_COLL(COLL_BGK) LBF_BATCH_CHUNK_COLL(COLL_TRT) LBF_BATCH_CHUNK_COLL(COLL_MRT) \
         return cudaErrorInvalidValue;                                                              \
     }                                                                                              \
     template <>                                                                                    \

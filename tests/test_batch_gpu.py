@@ -303,3 +303,27 @@ def test_batch_scalar_domain_needs_even_interval(env):
         d.init()
         with pytest.raises(RuntimeError, match="EUNSUPPORTED"):
             batch.admit(d, 100)
+
+
+def test_batch_chunk_launch_equals_step_launches(env):
+    """A group's chunk in one cooperative launch (grid barriers between the steps)
+    and one launch per step give the same bits and the same stop steps, for dense
+    and sparse groups, with domains joining late."""
+    Domain, Batch, _ = env
+    mix = [p for p, _ in _mix()]
+    got = []
+    for chunk in (1, 0):
+        with Batch(0, K) as batch:
+            batch.set_option(_abi.LBF_BATCH_OPT_CHUNK_LAUNCH, chunk)
+            live = {}
+            for i, p in enumerate(mix):
+                d = Domain(p).init()
+                if i % 2:
+                    d.step(3)          # joins at another phase
+                batch.admit(d, MAX_IT, 1e-7, 1e-7, 1e-7)
+                live[d.h.value] = i
+            got.append(_drain(batch, live))
+    a, b = got
+    for i in range(len(mix)):
+        assert a[i][0] == b[i][0] and a[i][3] == b[i][3], i
+        assert np.array_equal(a[i][1], b[i][1]) and np.array_equal(a[i][2], b[i][2]), i
