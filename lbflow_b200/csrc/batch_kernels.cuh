@@ -11,8 +11,9 @@
 // stopped, or whose next step is past its last one, costs its blocks one load
 // and an early exit.  The per-node work is the same code as the single-domain
 // sweep (process_cell), so a domain computes the same values alone and in a
-// batch.  Scalar domains are not batched.  Domains in the sparse (fluid-only)
-// layout form their own groups, swept by k_step_batch_sparse.
+// batch.  Domains with scalars or the central-moment collision run their own
+// single-domain sweep inside the batch's chunk graph instead.  Domains in the
+// sparse (fluid-only) layout form their own groups, swept by k_step_batch_sparse.
 #pragma once
 
 #include <cooperative_groups.h>
