@@ -92,6 +92,8 @@ def parse():
     ap.add_argument("--serve-mode", default="lanes", choices=["lanes", "single"],
                     help="serve: two batches (small requests on a high-priority stream) or one batch")
     ap.add_argument("--max-steps", type=int, default=2000, help="serve: steps per request at most")
+    ap.add_argument("--small-cap-busy", type=int, default=0,
+                    help="serve (lanes): small requests admitted at most while a large one runs (0: no cap)")
     ap.add_argument("--chunk", type=int, default=50, help="serve: residual interval (steps per chunk)")
     ap.add_argument("--no-sequential", action="store_true", help="serve: skip the one-at-a-time baseline")
     ap.add_argument("--seq-plain", action="store_true",
@@ -636,7 +638,8 @@ def run_serve(args, rank, world, local_rank):
     check = set(int(x) for x in rng.choice(f16, size=min(12, len(f16)), replace=False)) if f16 else set()
     with Clocks(local_rank) as clk:
         if args.serve_mode == "lanes":
-            rb = serve.serve_lanes(reqs, max_steps=args.max_steps, residual_interval=args.chunk, keep=check)
+            rb = serve.serve_lanes(reqs, max_steps=args.max_steps, residual_interval=args.chunk, keep=check,
+                                   small_cap_busy=args.small_cap_busy)
         else:
             rb = serve.serve_batched(reqs, max_steps=args.max_steps, residual_interval=args.chunk)
     sb = serve.summary(rb)

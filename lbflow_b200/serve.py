@@ -232,7 +232,8 @@ class _Arrivals:
 
 def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float = 1e-6,
                 residual_interval: int = 50, budget_bytes: int = 0, large_nodes: int = 1 << 19,
-                create_ms: float = 5.0, keep: Optional[set] = None, large_slots: int = 1) -> List[Record]:
+                create_ms: float = 5.0, keep: Optional[set] = None, large_slots: int = 1,
+                small_cap_busy: int = 0) -> List[Record]:
     """Run the requests through two batches ("lanes") that advance independently.
 
     Small requests (fewer than `large_nodes` nodes) go to a lane on a high-priority
@@ -245,6 +246,8 @@ def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float 
     boundaries and, between polls, builds the domains of arrived requests,
     smallest first, while the device-memory budget allows.  The stop rule, the
     fields and the step counts are those of `serve_batched` and `Domain.run`.
+    `small_cap_busy` > 0 admits at most that many small requests while a large
+    one runs (its share of the GPU sets the tail latency); 0: no cap.
     The velocity fields of the requests whose ids are in `keep` are kept in
     `serve_lanes.fields` (id -> (N, D) array).
     """
@@ -316,6 +319,8 @@ def serve_lanes(reqs: List[Request], max_steps: int = 2000, tol_velocity: float 
                         used -= r.est_bytes
                     ln["ev"] = None
                 cap = large_slots if li == 1 else len(ln["ready"]) + len(ln["live"])
+                if li == 0 and small_cap_busy > 0 and lanes[1]["live"]:
+                    cap = small_cap_busy
                 while ln["ready"] and len(ln["live"]) < cap:
                     r, dom = ln["ready"].pop(0)
                     ln["batch"].admit(dom, max_it, tol_density=math.inf, tol_velocity=tol_velocity,
