@@ -227,6 +227,14 @@ struct Store<ST_F16> {
     __device__ static __forceinline__ T enc_sr(R v, uint32_t r) {
         return __float2half_rz(__uint_as_float(__float_as_uint(v) + (r >> 19)));
     }
+    // two values with the conversion's own stochastic rounding (random bits r):
+    // .x = a, .y = b
+    __device__ static __forceinline__ void enc_sr2(R a, R b, uint32_t r, T& ta, T& tb) {
+        unsigned d;
+        asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(r));
+        ta = __ushort_as_half((unsigned short)(d >> 16));   // a goes to the upper half
+        tb = __ushort_as_half((unsigned short)(d & 0xffffu));
+    }
 };
 template <>
 struct Store<ST_BF16> {
@@ -241,6 +249,12 @@ struct Store<ST_BF16> {
     __device__ static __forceinline__ T enc(R v) { return __float2bfloat16_rn(v); }
     __device__ static __forceinline__ T enc_sr(R v, uint32_t r) {
         return __float2bfloat16_rz(__uint_as_float(__float_as_uint(v) + (r >> 16)));
+    }
+    __device__ static __forceinline__ void enc_sr2(R a, R b, uint32_t r, T& ta, T& tb) {
+        unsigned d;
+        asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(r));
+        ta = __ushort_as_bfloat16((unsigned short)(d >> 16));
+        tb = __ushort_as_bfloat16((unsigned short)(d & 0xffffu));
     }
 };
 
@@ -1003,6 +1017,19 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
 // Odd multipliers that spread a node's seed over its directions.
 __host__ __device__ constexpr uint32_t sr_mult(int i) { return 0x9e3779b1u + 0x632be5abu * (uint32_t)(2 * i); }
 
+// Two 16-bit directions i, j (neither the rest population) with stochastic
+// rounding by one paired conversion; returns the mass their rounding added.
+template <class S, int I, int J, class Put>
+__device__ __forceinline__ typename S::R store_pair_sr(typename S::R vi, typename S::R vj, uint32_t nseed,
+                                                       Put&& put) {
+    static_assert(I != 0 && J != 0, "the rest population is stored last, with the mass correction");
+    typename S::T ti, tj;
+    S::enc_sr2(vi, vj, nseed * sr_mult(I), ti, tj);
+    put(IC<I>{}, ti);
+    put(IC<J>{}, tj);
+    return (vi - S::cvt(ti)) + (vj - S::cvt(tj));
+}
+
 // `put(IC<i>, t)` stores the post-collision value of direction i, already in the
 // storage type.  `nseed` seeds the stochastic rounding of 16-bit storage.
 template <int VS, int COLL, int ST, class Put>
@@ -1089,8 +1116,15 @@ __device__ __forceinline__ void collide_store(const KParams<VS>& P, typename Sto
                     vi += cp * R(0.5) * (si + sb) + cm * R(0.5) * (si - sb);
                     vb += cp * R(0.5) * (sb + si) + cm * R(0.5) * (sb - si);
                 }
-                store(IC<i>{}, vi);
-                if constexpr (i != ib) store(IC<ib>{}, vb);
+                if constexpr (SIXTEEN && i != ib && i != 0) {
+                    // the pair rounded stochastically by one paired conversion
+                    // (cvt.rs on sm_100a), one random word per pair
+                    if (P.sround) merr += store_pair_sr<S, i, ib>(vi, vb, nseed, put);
+                    else { store(IC<i>{}, vi); store(IC<ib>{}, vb); }
+                } else {
+                    store(IC<i>{}, vi);
+                    if constexpr (i != ib) store(IC<ib>{}, vb);
+                }
             }
         });
     } else if constexpr (COLL == COLL_CENTRAL) {
