@@ -178,8 +178,9 @@ cudaError_t download(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     // page-locked caller memory (cudaMallocHost, cudaHostRegister, a pinned tensor):
     // one direct copy at the full link rate
     cudaPointerAttributes pa;
-    const bool pinned = cudaPointerGetAttributes(&pa, dst) == cudaSuccess && pa.type == cudaMemoryTypeHost;
-    if (!pinned) cudaGetLastError();   // pageable memory is not an error
+    const cudaError_t ea = cudaPointerGetAttributes(&pa, dst);
+    if (ea != cudaSuccess) cudaGetLastError();   // an unknown pointer is pageable memory, not an error
+    const bool pinned = ea == cudaSuccess && pa.type == cudaMemoryTypeHost;
     if (pinned || bytes < (4u << 20)) {
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
         return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
@@ -1240,7 +1241,10 @@ lbf_status do_steps(lbf_domain* D, long long nsteps, long long k, cudaStream_t s
         } else {
             e = launch_step_any(D, P, s);
         }
-        if (e != cudaSuccess) return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
+        if (e != cudaSuccess) {
+            if (ovl) cudaStreamSynchronize(D->side);   // nothing of this domain stays in flight on it
+            return fail(LBF_EDEVICE, std::string("step kernel: ") + cudaGetErrorString(e));
+        }
         if (P.residual) {
             k_finalize<<<1, FINALIZE_THREADS, 0, s>>>(D->accum, D->accum_cap, D->slot_next, D->nacc(), 1, D->res_dev);
             CK(cudaGetLastError());
