@@ -121,7 +121,12 @@ cudaError_t launch_sparse_st(KParams<VS>& kp, cudaStream_t stream) {
         case SWEEP_AA_EVEN: k_step_sparse<VS, COLL, ST, SWEEP_AA_EVEN><<<blocks, 256, 0, stream>>>(kp); break;
         case SWEEP_AA_ODD: k_step_sparse<VS, COLL, ST, SWEEP_AA_ODD><<<blocks, 256, 0, stream>>>(kp); break;
         case SWEEP_PUSH: k_step_sparse<VS, COLL, ST, SWEEP_PUSH><<<blocks, 256, 0, stream>>>(kp); break;
-        default: k_step_sparse<VS, COLL, ST, SWEEP_PULL><<<blocks, 256, 0, stream>>>(kp); break;
+        default:
+            if (!kp.first && !kp.observe && !kp.residual && !kp.write_mom)
+                k_step_sparse<VS, COLL, ST, SWEEP_PULL_PLAIN><<<blocks, 256, 0, stream>>>(kp);
+            else
+                k_step_sparse<VS, COLL, ST, SWEEP_PULL><<<blocks, 256, 0, stream>>>(kp);
+            break;
     }
     return cudaGetLastError();
 }

@@ -1228,7 +1228,9 @@ __host__ __device__ constexpr int racc_n() { return SCALAR ? 4 + NSMAX : 5; }
 // residual steps; `put` stores the post-collision populations (see
 // collide_store).  Returns the velocity (force-shifted) and its square, which
 // the scalars' equilibria use.
-template <int VS, int COLL, int ST, bool FACEBC, class MAdd, class Put>
+// OUT = false: a step without outputs (not the first step, no residual, moment
+// write or observation); those branches are then not compiled in.
+template <int VS, int COLL, int ST, bool FACEBC, bool OUT = true, class MAdd, class Put>
 __device__ __forceinline__ void momentum_cell(const KParams<VS>& P, const Geo& g, uint32_t mk,
                                               typename Store<ST>::R (&f)[Lat<VS>::Q], MAdd&& madd, Put&& put,
                                               typename Store<ST>::R (&u)[3], typename Store<ST>::R& uu) {
@@ -1271,12 +1273,12 @@ __device__ __forceinline__ void momentum_cell(const KParams<VS>& P, const Geo& g
     uu = R(0);
     sfor<D>([&](auto A) { uu += u[A] * u[A]; });
 
-    if (P.observe) {
+    if (OUT && P.observe) {
         P.obs_rho[g.cell] = double(rho);
         sfor<D>([&](auto A) { P.obs_u[(long long)g.cell * D + A] = double(u[A]); });
     } else {
         // ---- residual moments (src/momentum/lattice.rs:369-394) ------------------
-        if (P.residual) {
+        if (OUT && P.residual) {
             const R* mp = (const R*)P.mom_prev;
             const double d0 = double(rho) - double(mp[g.cell]);
             madd(IC<0>{}, d0 * d0);
@@ -1285,7 +1287,7 @@ __device__ __forceinline__ void momentum_cell(const KParams<VS>& P, const Geo& g
                 madd(IC<1 + int(A)>{}, du * du);
             });
         }
-        if (P.write_mom) {
+        if (OUT && P.write_mom) {
             R* mc = (R*)P.mom_cur;
             mc[g.cell] = rho;
             sfor<D>([&](auto A) { mc[(1 + A) * P.N + g.cell] = u[A]; });
@@ -1413,13 +1415,14 @@ __device__ __forceinline__ void scalar_cells(const KParams<VS>& P, const Geo& g,
 
 // Everything a fluid node does after its populations were pulled: the momentum
 // part, then the scalars.  Shared by every sweep.
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class Put, class GPull, int K>
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, bool OUT = true, class Put, class GPull, int K>
 __device__ __forceinline__ void process_cell_put(const KParams<VS>& P, const Geo& g, uint32_t mk,
                                                  typename Store<ST>::R (&f)[Lat<VS>::Q], double (&racc)[K],
                                                  Put&& put, GPull&& gpull) {
     using R = typename Store<ST>::R;
     R u[3], uu;
-    momentum_cell<VS, COLL, ST, FACEBC>(P, g, mk, f, [&](auto J, double v) { racc[int(J)] += v; }, put, u, uu);
+    momentum_cell<VS, COLL, ST, FACEBC, OUT>(P, g, mk, f, [&](auto J, double v) { racc[int(J)] += v; }, put, u,
+                                             uu);
     if constexpr (SCALAR) {
         // a static index keeps racc in registers
         auto radd = [&](int si, double v) {
@@ -1440,12 +1443,12 @@ struct NoScalarPull {
 // The A/B layouts: the post-collision populations go to slot `pidx` of the
 // destination planes (the node index for the dense layouts, the fluid-node index
 // for the sparse layout).
-template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, class GPull, int K>
+template <int VS, int COLL, int ST, bool FACEBC, bool SCALAR, bool OUT = true, class GPull, int K>
 __device__ __forceinline__ void process_cell_at(const KParams<VS>& P, const Geo& g, uint32_t mk,
                                                 typename Store<ST>::R (&f)[Lat<VS>::Q], double (&racc)[K],
                                                 long long pidx, GPull&& gpull) {
     using S = Store<ST>;
-    process_cell_put<VS, COLL, ST, FACEBC, SCALAR>(
+    process_cell_put<VS, COLL, ST, FACEBC, SCALAR, OUT>(
         P, g, mk, f, racc, [&](auto I, typename S::T v) { ((typename S::T*)P.dstp[I])[pidx] = v; }, gpull);
 }
 
@@ -1924,6 +1927,10 @@ __device__ __forceinline__ int sparse_source(const StepParams& P, const Geo& g, 
 // is solid), which is f_{t+1}.  The values and the arithmetic are again those of
 // the pull sweep.
 constexpr int SWEEP_PULL = 0, SWEEP_AA_EVEN = 1, SWEEP_AA_ODD = 2, SWEEP_PUSH = 3;
+// A kernel form, not a streaming scheme: the pull sweep of a step without outputs
+// (not the first step, no residual, moment write or observation), compiled
+// without those branches so that its body is shorter.
+constexpr int SWEEP_PULL_PLAIN = 4;
 
 // One fluid node of the sparse sweep (k64 = its fluid index; lanes past the
 // last fluid node only take part in the block reduction).  `e` and `mk` (its
@@ -2024,7 +2031,7 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
             ((T*)P.dstp[0])[off[L::qbar(I)]] = v;
         }, NoScalarPull{});
     } else {
-        if (P.first) {
+        if (MODE != SWEEP_PULL_PLAIN && P.first) {
             sfor<Q>([&](auto I) { f[I] = S::ld(P.srcp[I], k); });
         } else {
             // WRAP: the periodic wrap in x (x = 0 pulls from x = nx - 1 and x = nx - 1
@@ -2043,7 +2050,7 @@ __device__ __forceinline__ void sparse_node_at(const KParams<VS>& P, long long k
             if (__any_sync(__activemask(), g.x == 0 || g.x == P.nx - 1)) pull(IC<1>{});
             else pull(IC<0>{});
         }
-        process_cell_at<VS, COLL, ST, false, false>(P, g, mk, f, racc, k, NoScalarPull{});
+        process_cell_at<VS, COLL, ST, false, false, MODE != SWEEP_PULL_PLAIN>(P, g, mk, f, racc, k, NoScalarPull{});
     }
 }
 
@@ -2113,7 +2120,7 @@ __global__ void __launch_bounds__(256, (sparse_blocks<VS, COLL, ST, MODE>())) k_
     double racc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     const long long k = P.kbeg + blockIdx.x * (long long)blockDim.x + threadIdx.x;
     sparse_node<VS, COLL, ST, MODE>(P, k < P.kend ? k : P.nlist, racc);   // nlist: no update
-    if (P.residual && !P.observe) step_partials<5>(racc, P, blockIdx.x);
+    if (MODE != SWEEP_PULL_PLAIN && P.residual && !P.observe) step_partials<5>(racc, P, blockIdx.x);
 }
 
 // =================================================================== sparse sweep, faces and scalar
