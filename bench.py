@@ -147,18 +147,35 @@ class Clocks:
         self.path = os.path.join(tempfile.gettempdir(), f"lbf_clocks_{os.getpid()}.csv")
         self.proc = None
 
+    def _lines(self) -> int:
+        try:
+            with open(self.path) as fh:
+                return sum(1 for _ in fh)
+        except OSError:
+            return 0
+
+    def _wait_lines(self, n: int, limit_s: float) -> None:
+        t_end = time.perf_counter() + limit_s
+        while self._lines() < n and time.perf_counter() < t_end and self.proc.poll() is None:
+            time.sleep(0.01)
+
     def __enter__(self):
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            # the sampler is running (its first line written) when the timed region starts
+            self._wait_lines(1, 3.0)
         except Exception:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            # a timed region shorter than the sampling period still gets the sample
+            # that follows it
+            self._wait_lines(2, 0.5)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
