@@ -369,8 +369,12 @@ lbf_status lbf_format_coordinates(const int64_t* n, int32_t d, double delta_x, c
  * launch per time step, and a chunk of `residual_interval` = k steps plus an
  * on-device residual + stop-rule evaluation is captured once as a CUDA graph and
  * replayed.  Each domain stops exactly where lbf_domain_run(max_iterations, k,
- * tol_*) would stop it, with the same fields.  Domains with a scalar are not
- * batched (LBF_EUNSUPPORTED).  While admitted, a domain refuses the standalone
+ * tol_*) would stop it, with the same fields.  Domains with scalars, the
+ * central-moment collision or the sparse layout with explicit faces run their
+ * own single-domain sweep inside the chunk graph: they are admitted only with an
+ * even residual_interval and without the pipelined or staged sweep
+ * (LBF_EUNSUPPORTED otherwise); z-slab domains are not batched.  While admitted,
+ * a domain refuses the standalone
  * calls (LBF_ESTATE); lbf_batch_poll hands it back once it stopped, and
  * lbf_domain_destroy evicts it first.  The batch object is thread-safe.
  *
